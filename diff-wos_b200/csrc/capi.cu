@@ -1,0 +1,408 @@
+// extern "C" entry points of libwos_b200.so (declared in include/wos_b200.h).
+#include <cstring>
+#include <string>
+
+#include "../../include/wos_b200.h"
+#include "scene_impl.h"
+#include "walk.h"
+
+namespace wosd {
+
+static thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int fail_cuda(cudaError_t e, const char *where) {
+    g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
+    return WOS_ERR_CUDA;
+}
+
+static bool is_device_ptr(const void *p) {
+    if (p == nullptr) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+#define WOS_CHECK_DEV(ptr, name)                                                              \
+    do {                                                                                      \
+        if (!is_device_ptr(ptr))                                                              \
+            return fail(WOS_ERR_INVALID_ARGUMENT, std::string(name) + " must be a device pointer"); \
+    } while (0)
+
+#define WOS_CHECK_DEV_OPT(ptr, name)            \
+    do {                                        \
+        if ((ptr) != nullptr) WOS_CHECK_DEV(ptr, name); \
+    } while (0)
+
+static int check_params(const wos_params *p) {
+    if (p == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "params is NULL");
+    if (p->nwalks < 1) return fail(WOS_ERR_INVALID_ARGUMENT, "nwalks must be >= 1");
+    if (p->nsteps < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "nsteps must be >= 0");
+    if (!(p->epsilon >= 0.0f)) return fail(WOS_ERR_INVALID_ARGUMENT, "epsilon must be >= 0");
+    return 0;
+}
+
+static int check_adj(const wos_adjoint_params *a) {
+    if (a == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "adjoint params is NULL");
+    if (!(a->epsilon2 >= 0.0f)) return fail(WOS_ERR_INVALID_ARGUMENT, "epsilon2 must be >= 0");
+    if (!(a->clamping >= 0.0f)) return fail(WOS_ERR_INVALID_ARGUMENT, "clamping must be >= 0");
+    return 0;
+}
+
+static AdjCfg make_adj(const wos_adjoint_params &a) {
+    AdjCfg c;
+    c.epsilon2 = a.epsilon2;
+    c.clamping = a.clamping;
+    c.control_variates = a.control_variates;
+    c.source_in_nd = a.source_in_normal_derivative;
+    c.ball_eps = a.ball_epsilon;
+    c.want_dV = a.want_dV;
+    c.want_dg = a.want_dg;
+    c.want_dsrc = a.want_dsrc;
+    return c;
+}
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Stream-ordered scratch that is either carved from the caller's workspace
+// or allocated (and freed) on the stream.
+struct Scratch {
+    char *base = nullptr;
+    bool owned = false;
+    cudaStream_t st = nullptr;
+    int init(void *ws, size_t ws_bytes, size_t need, cudaStream_t s) {
+        st = s;
+        if (ws != nullptr) {
+            if (ws_bytes < need) return fail(WOS_ERR_WORKSPACE, "workspace too small");
+            if (!is_device_ptr(ws)) return fail(WOS_ERR_INVALID_ARGUMENT, "workspace must be a device pointer");
+            base = (char *)ws;
+            return 0;
+        }
+        const cudaError_t e = cudaMallocAsync((void **)&base, need ? need : 256, s);
+        if (e != cudaSuccess) return fail_cuda(e, "cudaMallocAsync(workspace)");
+        owned = true;
+        return 0;
+    }
+    ~Scratch() {
+        if (owned && base) cudaFreeAsync(base, st);
+    }
+};
+
+}  // namespace wosd
+
+using namespace wosd;
+
+extern "C" {
+
+int wos_version(void) { return 100; }
+
+const char *wos_last_error_string(void) { return g_last_error.c_str(); }
+
+int wos_device_status(int reset, int32_t *out) {
+    if (out == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "out is NULL");
+    int v = 0;
+    const int rc = read_status(reset, &v);
+    *out = v;
+    return rc;
+}
+
+int wos_scene_create(int dim, const float *V, int nV, const int *F, int nF, const float *g, int source_type,
+                     const float *source_params, wos_stream_t stream, wos_scene_t *out) {
+    if (out == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (dim != 2 && dim != 3) return fail(WOS_ERR_INVALID_ARGUMENT, "dim must be 2 or 3");
+    if (nV < 1 || nF < 1) return fail(WOS_ERR_EMPTY_SCENE, "scene needs at least one vertex and one face");
+    if (source_type < 0 || source_type > 2) return fail(WOS_ERR_INVALID_ARGUMENT, "source_type must be 0, 1 or 2");
+    if (dim == 3 && source_type != 0) return fail(WOS_ERR_UNSUPPORTED, "3D scenes have no source term");
+    if (source_type != 0 && source_params == nullptr)
+        return fail(WOS_ERR_INVALID_ARGUMENT, "source_params is NULL for a source");
+    WOS_CHECK_DEV(V, "V");
+    WOS_CHECK_DEV(F, "F");
+    WOS_CHECK_DEV(g, "g");
+    cudaStream_t st = (cudaStream_t)stream;
+    wos_scene_s *s = new wos_scene_s();
+    SceneImpl &S = s->impl;
+    S.dim = dim;
+    S.nV = nV;
+    S.nF = nF;
+    cudaGetDevice(&S.device);
+    S.src_type = source_type;
+    for (int k = 0; k < 5; ++k) S.src[k] = source_type ? source_params[k] : 0.0f;
+    int rc = S.allocate(st);
+    if (!rc) {
+        cudaError_t e = cudaMemcpyAsync(S.V, V, sizeof(float) * nV * dim, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(S.F, F, sizeof(int) * nF * dim, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(S.g, g, sizeof(float) * nV, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) rc = fail_cuda(e, "cudaMemcpyAsync(scene inputs)");
+    }
+    if (!rc) rc = S.check_indices(st);
+    if (!rc) rc = S.build(st);
+    if (rc) {
+        S.release(st);
+        cudaStreamSynchronize(st);
+        delete s;
+        return rc;
+    }
+    *out = s;
+    return 0;
+}
+
+int wos_scene_destroy(wos_scene_t scene, wos_stream_t stream) {
+    if (scene == nullptr) return 0;
+    scene->impl.release((cudaStream_t)stream);
+    delete scene;
+    return 0;
+}
+
+int wos_scene_update_values(wos_scene_t scene, const float *g, wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    WOS_CHECK_DEV(g, "g");
+    SceneImpl &S = scene->impl;
+    const cudaError_t e =
+        cudaMemcpyAsync(S.g, g, sizeof(float) * S.nV, cudaMemcpyDeviceToDevice, (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpyAsync(values)");
+    return 0;
+}
+
+int wos_scene_update_vertices(wos_scene_t scene, const float *V, wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    WOS_CHECK_DEV(V, "V");
+    SceneImpl &S = scene->impl;
+    cudaStream_t st = (cudaStream_t)stream;
+    const cudaError_t e = cudaMemcpyAsync(S.V, V, sizeof(float) * S.nV * S.dim, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpyAsync(vertices)");
+    return S.build(st);
+}
+
+int wos_scene_set_source(wos_scene_t scene, int source_type, const float *params) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (source_type < 0 || source_type > 2) return fail(WOS_ERR_INVALID_ARGUMENT, "source_type must be 0, 1 or 2");
+    SceneImpl &S = scene->impl;
+    if (S.dim == 3 && source_type != 0) return fail(WOS_ERR_UNSUPPORTED, "3D scenes have no source term");
+    if (source_type != 0 && params == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "params is NULL");
+    S.src_type = source_type;
+    for (int k = 0; k < 5; ++k) S.src[k] = source_type ? params[k] : 0.0f;
+    return 0;
+}
+
+int wos_scene_get_info(wos_scene_t scene, wos_scene_info *out) {
+    if (scene == nullptr || out == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "NULL argument");
+    const SceneImpl &S = scene->impl;
+    out->dim = S.dim;
+    out->n_vertices = S.nV;
+    out->n_faces = S.nF;
+    out->n_nodes = S.nNodes;
+    out->bvh_depth = S.depth;
+    out->source_type = S.src_type;
+    for (int k = 0; k < 3; ++k) {
+        out->aabb_min[k] = S.lo[k];
+        out->aabb_max[k] = S.hi[k];
+    }
+    for (int k = 0; k < 5; ++k) out->source_params[k] = S.src[k];
+    return 0;
+}
+
+int wos_scene_get_normals(wos_scene_t scene, float *out, wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    WOS_CHECK_DEV(out, "out");
+    const SceneImpl &S = scene->impl;
+    const cudaError_t e =
+        cudaMemcpyAsync(out, S.N, sizeof(float) * S.nV * S.dim, cudaMemcpyDeviceToDevice, (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpyAsync(normals)");
+    return 0;
+}
+
+int wos_closest_point(wos_scene_t scene, const float *P, int n, int use_bvh, int32_t *prim, float *dist,
+                      float *t_or_uv, float *pt, float *normal, float *sdf, uint8_t *inside, wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (n < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "n must be >= 0");
+    if (n == 0) return 0;
+    WOS_CHECK_DEV(P, "P");
+    WOS_CHECK_DEV_OPT(prim, "prim");
+    WOS_CHECK_DEV_OPT(dist, "dist");
+    WOS_CHECK_DEV_OPT(t_or_uv, "t_or_uv");
+    WOS_CHECK_DEV_OPT(pt, "pt");
+    WOS_CHECK_DEV_OPT(normal, "normal");
+    WOS_CHECK_DEV_OPT(sdf, "sdf");
+    WOS_CHECK_DEV_OPT(inside, "inside");
+    QueryOut o{prim, dist, t_or_uv, pt, normal, sdf, inside};
+    return launch_closest(scene->impl, P, n, use_bvh != 0, o, (cudaStream_t)stream);
+}
+
+int wos_largest_inscribed_ball(wos_scene_t scene, const uint8_t *valid, const float *pt, const float *normal, int n,
+                               float epsilon, int use_bvh, float *R, wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (n < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "n must be >= 0");
+    if (n == 0) return 0;
+    WOS_CHECK_DEV(valid, "valid");
+    WOS_CHECK_DEV(pt, "pt");
+    WOS_CHECK_DEV(normal, "normal");
+    WOS_CHECK_DEV(R, "R");
+    return launch_ball(scene->impl, valid, pt, normal, n, epsilon, use_bvh != 0, R, (cudaStream_t)stream);
+}
+
+int wos_walk_records(wos_scene_t scene, const float *P, int n, const wos_params *p, uint8_t *valid, float *pt,
+                     float *normal, float *t_or_uv, int32_t *prim, float *contrib, wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (int rc = check_params(p)) return rc;
+    if (n < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "n must be >= 0");
+    if (n == 0) return 0;
+    WOS_CHECK_DEV(P, "P");
+    WOS_CHECK_DEV(valid, "valid");
+    WOS_CHECK_DEV_OPT(pt, "pt");
+    WOS_CHECK_DEV_OPT(normal, "normal");
+    WOS_CHECK_DEV_OPT(t_or_uv, "t_or_uv");
+    WOS_CHECK_DEV_OPT(prim, "prim");
+    WOS_CHECK_DEV_OPT(contrib, "contrib");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch s;
+    if (int rc = s.init(nullptr, 0, 256, st)) return rc;
+    WalkOut o{nullptr, nullptr, valid, pt, normal, t_or_uv, prim, contrib};
+    return launch_walk(scene->impl, P, n, *p, true, o, (unsigned long long *)s.base, st);
+}
+
+int wos_walk_values(wos_scene_t scene, const float *P, int n, const wos_params *p, float *values, int32_t *steps,
+                    wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (int rc = check_params(p)) return rc;
+    if (n < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "n must be >= 0");
+    if (n == 0) return 0;
+    WOS_CHECK_DEV(P, "P");
+    WOS_CHECK_DEV(values, "values");
+    WOS_CHECK_DEV_OPT(steps, "steps");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch s;
+    if (int rc = s.init(nullptr, 0, 256, st)) return rc;
+    WalkOut o{values, steps, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    return launch_walk(scene->impl, P, (long long)n * p->nwalks, *p, false, o, (unsigned long long *)s.base, st);
+}
+
+int wos_walk_values_plain(wos_scene_t scene, const float *P, int n, const wos_params *p, float *values,
+                          wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (int rc = check_params(p)) return rc;
+    if (n < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "n must be >= 0");
+    if (n == 0) return 0;
+    WOS_CHECK_DEV(P, "P");
+    WOS_CHECK_DEV(values, "values");
+    return launch_walk_plain(scene->impl, P, (long long)n * p->nwalks, *p, values, (cudaStream_t)stream);
+}
+
+size_t wos_solve_workspace_size(int n, const wos_params *p) {
+    if (p == nullptr || n < 0 || p->nwalks < 1) return 0;
+    return 256 + align256(sizeof(float) * (size_t)n * (size_t)p->nwalks);
+}
+
+int wos_solve(wos_scene_t scene, const float *P, int n, const wos_params *p, double *mean, double *var,
+              void *workspace, size_t workspace_bytes, wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (int rc = check_params(p)) return rc;
+    if (n < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "n must be >= 0");
+    if (n == 0) return 0;
+    WOS_CHECK_DEV(P, "P");
+    WOS_CHECK_DEV(mean, "mean");
+    WOS_CHECK_DEV_OPT(var, "var");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch s;
+    if (int rc = s.init(workspace, workspace_bytes, wos_solve_workspace_size(n, p), st)) return rc;
+    unsigned long long *counter = (unsigned long long *)s.base;
+    float *vals = (float *)(s.base + 256);
+    WalkOut o{vals, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    if (int rc = launch_walk(scene->impl, P, (long long)n * p->nwalks, *p, false, o, counter, st)) return rc;
+    return launch_reduce(vals, n, p->nwalks, mean, var, st);
+}
+
+int wos_normal_derivative(wos_scene_t scene, const uint8_t *valid, const float *pt, const float *normal,
+                          const float *t_or_uv, const int32_t *prim, int n, const wos_params *p,
+                          const wos_adjoint_params *a, float *out, wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (int rc = check_params(p)) return rc;
+    if (int rc = check_adj(a)) return rc;
+    if (n < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "n must be >= 0");
+    if (n == 0) return 0;
+    WOS_CHECK_DEV(valid, "valid");
+    WOS_CHECK_DEV(pt, "pt");
+    WOS_CHECK_DEV(normal, "normal");
+    WOS_CHECK_DEV(t_or_uv, "t_or_uv");
+    WOS_CHECK_DEV(prim, "prim");
+    WOS_CHECK_DEV(out, "out");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch s;
+    if (int rc = s.init(nullptr, 0, 256, st)) return rc;
+    AdjOut o{};
+    o.rvalid = valid;
+    o.rpt = pt;
+    o.rnrm = normal;
+    o.rtuv = t_or_uv;
+    o.rprim = prim;
+    o.nd = out;
+    return launch_adjoint(scene->impl, nullptr, n, *p, make_adj(*a), nullptr, true, o, (unsigned long long *)s.base,
+                          st);
+}
+
+size_t wos_adjoint_workspace_size(wos_scene_t scene) {
+    if (scene == nullptr) return 0;
+    const SceneImpl &S = scene->impl;
+    return 256 + align256(sizeof(double) * (size_t)S.nV * S.dim) + align256(sizeof(double) * (size_t)S.nV) + 256;
+}
+
+int wos_adjoint(wos_scene_t scene, const float *P, int n, const wos_params *p, const wos_adjoint_params *a,
+                const float *dLdu, float *dV, float *dg, float *dsrc, void *workspace, size_t workspace_bytes,
+                wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (int rc = check_params(p)) return rc;
+    if (int rc = check_adj(a)) return rc;
+    if (n < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "n must be >= 0");
+    if (n == 0) return 0;
+    if (a->want_dV && dV == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "want_dV set but dV is NULL");
+    if (a->want_dg && dg == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "want_dg set but dg is NULL");
+    if (a->want_dsrc && dsrc == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "want_dsrc set but dsrc is NULL");
+    WOS_CHECK_DEV(P, "P");
+    WOS_CHECK_DEV(dLdu, "dLdu");
+    WOS_CHECK_DEV_OPT(dV, "dV");
+    WOS_CHECK_DEV_OPT(dg, "dg");
+    WOS_CHECK_DEV_OPT(dsrc, "dsrc");
+    const SceneImpl &S = scene->impl;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t need = wos_adjoint_workspace_size(scene);
+    Scratch s;
+    if (int rc = s.init(workspace, workspace_bytes, need, st)) return rc;
+    unsigned long long *counter = (unsigned long long *)s.base;
+    double *aV = (double *)(s.base + 256);
+    double *ag = (double *)((char *)aV + align256(sizeof(double) * (size_t)S.nV * S.dim));
+    double *as = (double *)((char *)ag + align256(sizeof(double) * (size_t)S.nV));
+    cudaError_t e = cudaMemsetAsync(s.base, 0, need, st);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(adjoint workspace)");
+    AdjOut o{};
+    o.dV = aV;
+    o.dg = ag;
+    o.dsrc = as;
+    if (int rc = launch_adjoint(S, P, (long long)n * p->nwalks, *p, make_adj(*a), dLdu, false, o, counter, st))
+        return rc;
+    if (a->want_dV)
+        if (int rc = launch_add_f64(aV, dV, (long long)S.nV * S.dim, st)) return rc;
+    if (a->want_dg)
+        if (int rc = launch_add_f64(ag, dg, S.nV, st)) return rc;
+    if (a->want_dsrc)
+        if (int rc = launch_add_f64(as, dsrc, 5, st)) return rc;
+    return 0;
+}
+
+int wos_set_launch_config(int dim, const wos_launch_config *cfg) {
+    if (cfg == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "cfg is NULL");
+    return set_launch_config(dim, cfg);
+}
+
+int wos_get_launch_config(int dim, wos_launch_config *out) {
+    if (out == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "out is NULL");
+    return get_launch_config(dim, out);
+}
+
+}  // extern "C"

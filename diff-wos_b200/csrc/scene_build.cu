@@ -1,0 +1,619 @@
+// Scene construction on the GPU: vertex normals, scene AABB, primitive
+// precomputation and the LBVH (Morton codes, radix sort, Karras hierarchy,
+// bottom-up refit, breadth-first node order).
+//
+// Replaces the reference's host Scene<N>::configure_normal / configure
+// (include/scene.cuh:368-453), which did the AABB on the host and the BVH in
+// the third-party lbvh library.  Everything here is deterministic: vertex
+// normals are summed per vertex in (face, slot) order, the tree is a pure
+// function of the sorted (morton << 32 | prim) keys, and boxes are min/max.
+#include <cub/cub.cuh>
+
+#include <vector>
+
+#include "scene_impl.h"
+#include "wos_device.cuh"
+
+namespace wosd {
+
+#define WOS_TRY(x)                                    \
+    do {                                              \
+        cudaError_t _e = (x);                         \
+        if (_e != cudaSuccess) return fail_cuda(_e, #x); \
+    } while (0)
+
+// ------------------------------------------------------------------ kernels
+__device__ __forceinline__ int ordered_int(float f) {
+    int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float from_ordered_int(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+__global__ void k_check_indices(const int *F, long long n, int nV, int *bad) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int v = F[i];
+        if (v < 0 || v >= nV) atomicOr(bad, 1);
+    }
+}
+
+__global__ void k_aabb(const float *V, int nV, int dim, int *lohi) {
+    // lohi[0..2] = ordered min, lohi[3..5] = ordered max
+    __shared__ int smin[3], smax[3];
+    if (threadIdx.x < 3) {
+        smin[threadIdx.x] = 0x7fffffff;
+        smax[threadIdx.x] = (int)0x80000000;
+    }
+    __syncthreads();
+    int lmin[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, lmax[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nV; v += gridDim.x * blockDim.x)
+        for (int k = 0; k < dim; ++k) {
+            const int o = ordered_int(V[(size_t)v * dim + k]);
+            lmin[k] = min(lmin[k], o);
+            lmax[k] = max(lmax[k], o);
+        }
+    for (int k = 0; k < dim; ++k) {
+        atomicMin(&smin[k], lmin[k]);
+        atomicMax(&smax[k], lmax[k]);
+    }
+    __syncthreads();
+    if (threadIdx.x < dim) {
+        atomicMin(&lohi[threadIdx.x], smin[threadIdx.x]);
+        atomicMax(&lohi[3 + threadIdx.x], smax[threadIdx.x]);
+    }
+}
+
+// Per (face, slot) normal contribution and its sort key (vertex << 32 | slot id).
+template <int D>
+__global__ void k_face_normals(const float *V, const int *F, int nF, float *contrib, unsigned long long *keys) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    if (D == 2) {
+        const int i0 = F[2 * f], i1 = F[2 * f + 1];
+        const float dx = V[2 * i1] - V[2 * i0], dy = V[2 * i1 + 1] - V[2 * i0 + 1];
+        float nx = dy, ny = -dx;
+        const float len = sqrtf(dot2(nx, ny, nx, ny));
+        if (len > 0.0f) {
+            nx = nx / len;
+            ny = ny / len;
+        } else {
+            nx = ny = 0.0f;
+        }
+        for (int s = 0; s < 2; ++s) {
+            contrib[(size_t)(2 * f + s) * 2] = nx;
+            contrib[(size_t)(2 * f + s) * 2 + 1] = ny;
+            keys[2 * f + s] = ((unsigned long long)(unsigned)F[2 * f + s] << 32) | (unsigned)(2 * f + s);
+        }
+    } else {
+        const int i0 = F[3 * f], i1 = F[3 * f + 1], i2 = F[3 * f + 2];
+        const float *p0 = V + 3 * (size_t)i0, *p1 = V + 3 * (size_t)i1, *p2 = V + 3 * (size_t)i2;
+        float e10[3], e20[3], e21[3], e01[3], e02[3], e12[3];
+        for (int k = 0; k < 3; ++k) {
+            e10[k] = p1[k] - p0[k];
+            e20[k] = p2[k] - p0[k];
+            e21[k] = p2[k] - p1[k];
+            e01[k] = p0[k] - p1[k];
+            e02[k] = p0[k] - p2[k];
+            e12[k] = p1[k] - p2[k];
+        }
+        float n[3];
+        cross3(e10[0], e10[1], e10[2], e20[0], e20[1], e20[2], n[0], n[1], n[2]);
+        const float len = sqrtf(dot3(n[0], n[1], n[2], n[0], n[1], n[2]));
+        if (len > 0.0f) {
+            for (int k = 0; k < 3; ++k) n[k] = n[k] / len;
+        } else {
+            n[0] = n[1] = n[2] = 0.0f;
+        }
+        auto angle = [](const float *a, const float *b) {
+            float c[3];
+            cross3(a[0], a[1], a[2], b[0], b[1], b[2], c[0], c[1], c[2]);
+            return wosm::atan2_(sqrtf(dot3(c[0], c[1], c[2], c[0], c[1], c[2])), dot3(a[0], a[1], a[2], b[0], b[1], b[2]));
+        };
+        const float ang[3] = {angle(e10, e20), angle(e21, e01), angle(e02, e12)};
+        for (int s = 0; s < 3; ++s) {
+            for (int k = 0; k < 3; ++k) contrib[(size_t)(3 * f + s) * 3 + k] = ang[s] * n[k];
+            keys[3 * f + s] = ((unsigned long long)(unsigned)F[3 * f + s] << 32) | (unsigned)(3 * f + s);
+        }
+    }
+}
+
+__global__ void k_segments(const unsigned long long *keys, int n, int *beg, int *end) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned v = (unsigned)(keys[i] >> 32);
+    if (i == 0 || (unsigned)(keys[i - 1] >> 32) != v) beg[v] = i;
+    if (i == n - 1 || (unsigned)(keys[i + 1] >> 32) != v) end[v] = i + 1;
+}
+
+template <int D>
+__global__ void k_vertex_normals(const unsigned long long *keys, const float *contrib, const int *beg, const int *end,
+                                 int nV, float *N) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nV) return;
+    float s[3] = {0.0f, 0.0f, 0.0f};
+    for (int i = beg[v]; i < end[v]; ++i) {
+        const unsigned slot = (unsigned)keys[i];
+        for (int k = 0; k < D; ++k) s[k] += contrib[(size_t)slot * D + k];
+    }
+    const float len = sqrtf(D == 2 ? dot2(s[0], s[1], s[0], s[1]) : dot3(s[0], s[1], s[2], s[0], s[1], s[2]));
+    for (int k = 0; k < D; ++k) N[(size_t)v * D + k] = len > 0.0f ? s[k] / len : 0.0f;
+}
+
+__device__ __forceinline__ uint32_t spread2(uint32_t x) {
+    x &= 0xffffu;
+    x = (x | (x << 8)) & 0x00ff00ffu;
+    x = (x | (x << 4)) & 0x0f0f0f0fu;
+    x = (x | (x << 2)) & 0x33333333u;
+    x = (x | (x << 1)) & 0x55555555u;
+    return x;
+}
+__device__ __forceinline__ uint32_t spread3(uint32_t x) {
+    x &= 0x3ffu;
+    x = (x | (x << 16)) & 0x030000ffu;
+    x = (x | (x << 8)) & 0x0300f00fu;
+    x = (x | (x << 4)) & 0x030c30c3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+// Primitive precomputation, primitive boxes and Morton keys.
+template <int D>
+__global__ void k_prims(const float *V, const int *F, int nF, float lo0, float lo1, float lo2, float hi0, float hi1,
+                        float hi2, float4 *seg, float *seginv, float4 *tri, float *pbox, unsigned long long *keys) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    const float slo[3] = {lo0, lo1, lo2}, shi[3] = {hi0, hi1, hi2};
+    float bl[3], bh[3];
+    if (D == 2) {
+        const int i0 = F[2 * f], i1 = F[2 * f + 1];
+        const float ax = V[2 * i0], ay = V[2 * i0 + 1], bx = V[2 * i1], by = V[2 * i1 + 1];
+        const float bax = bx - ax, bay = by - ay;
+        const float len2 = dot2(bax, bay, bax, bay);
+        seg[f] = make_float4(ax, ay, bax, bay);
+        seginv[f] = len2 > 0.0f ? 1.0f / len2 : 0.0f;
+        bl[0] = fminf(ax, bx);
+        bh[0] = fmaxf(ax, bx);
+        bl[1] = fminf(ay, by);
+        bh[1] = fmaxf(ay, by);
+    } else {
+        const int i0 = F[3 * f], i1 = F[3 * f + 1], i2 = F[3 * f + 2];
+        float a[3], b[3], c[3];
+        for (int k = 0; k < 3; ++k) {
+            a[k] = V[3 * (size_t)i0 + k];
+            b[k] = V[3 * (size_t)i1 + k];
+            c[k] = V[3 * (size_t)i2 + k];
+        }
+        float ab[3], ac[3];
+        for (int k = 0; k < 3; ++k) {
+            ab[k] = b[k] - a[k];
+            ac[k] = c[k] - a[k];
+        }
+        tri[3 * f] = make_float4(a[0], a[1], a[2], dot3(ab[0], ab[1], ab[2], ab[0], ab[1], ab[2]));
+        tri[3 * f + 1] = make_float4(ab[0], ab[1], ab[2], dot3(ab[0], ab[1], ab[2], ac[0], ac[1], ac[2]));
+        tri[3 * f + 2] = make_float4(ac[0], ac[1], ac[2], dot3(ac[0], ac[1], ac[2], ac[0], ac[1], ac[2]));
+        for (int k = 0; k < 3; ++k) {
+            bl[k] = fminf(fminf(a[k], b[k]), c[k]);
+            bh[k] = fmaxf(fmaxf(a[k], b[k]), c[k]);
+        }
+    }
+    uint32_t q[3];
+    const float scale = D == 2 ? 65536.0f : 1024.0f;
+    for (int k = 0; k < D; ++k) {
+        pbox[(size_t)f * 2 * D + k] = bl[k];
+        pbox[(size_t)f * 2 * D + D + k] = bh[k];
+        const float c = (bl[k] + bh[k]) * 0.5f;
+        const float ext = shi[k] - slo[k];
+        const float u = ext > 0.0f ? (c - slo[k]) / ext : 0.0f;
+        q[k] = (uint32_t)fminf(fmaxf(u * scale, 0.0f), scale - 1.0f);
+    }
+    const uint32_t m = D == 2 ? (spread2(q[0]) | (spread2(q[1]) << 1))
+                              : (spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2));
+    keys[f] = ((unsigned long long)m << 32) | (unsigned)f;
+}
+
+__device__ __forceinline__ int kdelta(const unsigned long long *k, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    return __clzll(k[i] ^ k[j]);
+}
+
+// Karras 2012, one thread per internal node.
+__global__ void k_karras(const unsigned long long *k, int n, int2 *child, int *parent_int, int *parent_leaf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int d = (kdelta(k, n, i, i + 1) - kdelta(k, n, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = kdelta(k, n, i, i - d);
+    int lmax = 2;
+    while (kdelta(k, n, i, i + lmax * d) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+        if (kdelta(k, n, i, i + (l + t) * d) > dmin) l += t;
+    const int j = i + l * d;
+    const int dnode = kdelta(k, n, i, j);
+    int s = 0;
+    for (int div = 2;; div *= 2) {
+        const int t = (l + div - 1) / div;
+        if (kdelta(k, n, i, i + (s + t) * d) > dnode) s += t;
+        if (t == 1) break;
+    }
+    const int gamma = i + s * d + min(d, 0);
+    int2 c;
+    if (min(i, j) == gamma) {
+        c.x = ~gamma;
+        parent_leaf[gamma] = i;
+    } else {
+        c.x = gamma;
+        parent_int[gamma] = i;
+    }
+    if (max(i, j) == gamma + 1) {
+        c.y = ~(gamma + 1);
+        parent_leaf[gamma + 1] = i;
+    } else {
+        c.y = gamma + 1;
+        parent_int[gamma + 1] = i;
+    }
+    child[i] = c;
+}
+
+// Bottom-up boxes: the second thread to reach a node merges its children.
+template <int D>
+__global__ void k_refit(const unsigned long long *keys, int n, const float *pbox, const int2 *child,
+                        const int *parent_int, const int *parent_leaf, int *flags, float *nbox) {
+    const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (leaf >= n) return;
+    int v = parent_leaf[leaf];
+    while (v >= 0) {
+        __threadfence();
+        if (atomicAdd(&flags[v], 1) == 0) return;
+        __threadfence();
+        const int2 c = child[v];
+        float lo[3], hi[3];
+        for (int side = 0; side < 2; ++side) {
+            const int r = side == 0 ? c.x : c.y;
+            const float *b;
+            if (r < 0) {
+                const unsigned prim = (unsigned)keys[~r];
+                b = pbox + (size_t)prim * 2 * D;
+            } else {
+                b = nbox + (size_t)r * 2 * D;
+            }
+            for (int k = 0; k < D; ++k) {
+                const float l = __ldcg(b + k), h = __ldcg(b + D + k);
+                lo[k] = side == 0 ? l : fminf(lo[k], l);
+                hi[k] = side == 0 ? h : fmaxf(hi[k], h);
+            }
+        }
+        for (int k = 0; k < D; ++k) {
+            __stcg(nbox + (size_t)v * 2 * D + k, lo[k]);
+            __stcg(nbox + (size_t)v * 2 * D + D + k, hi[k]);
+        }
+        v = parent_int[v];
+    }
+}
+
+__global__ void k_depth(const int *parent_int, int nInt, unsigned long long *dkeys, int *maxdepth) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nInt) return;
+    int d = 0, v = i;
+    while (v > 0 && d < 4096) {
+        v = parent_int[v];
+        ++d;
+    }
+    dkeys[i] = ((unsigned long long)d << 32) | (unsigned)i;
+    atomicMax(maxdepth, d);
+}
+
+__global__ void k_bfs_rank(const unsigned long long *sorted, int nInt, int *new_of_old) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nInt) return;
+    new_of_old[(unsigned)sorted[r]] = r;
+}
+
+template <int D>
+__global__ void k_write_nodes(const unsigned long long *keys, int nInt, const float *pbox, const float *nbox,
+                              const int2 *child, const int *new_of_old, float4 *node) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nInt) return;
+    const int2 c = child[i];
+    float lo[2][3], hi[2][3];
+    int ref[2];
+    for (int side = 0; side < 2; ++side) {
+        const int r = side == 0 ? c.x : c.y;
+        const float *b;
+        if (r < 0) {
+            b = pbox + (size_t)(unsigned)keys[~r] * 2 * D;
+            ref[side] = r;
+        } else {
+            b = nbox + (size_t)r * 2 * D;
+            ref[side] = new_of_old[r];
+        }
+        for (int k = 0; k < D; ++k) {
+            lo[side][k] = b[k];
+            hi[side][k] = b[D + k];
+        }
+    }
+    const int o = new_of_old[i];
+    if (D == 2) {
+        node[3 * o] = make_float4(lo[0][0], lo[0][1], hi[0][0], hi[0][1]);
+        node[3 * o + 1] = make_float4(lo[1][0], lo[1][1], hi[1][0], hi[1][1]);
+        node[3 * o + 2] = make_float4(__int_as_float(ref[0]), __int_as_float(ref[1]), 0.0f, 0.0f);
+    } else {
+        node[4 * o] = make_float4(lo[0][0], lo[0][1], lo[0][2], hi[0][0]);
+        node[4 * o + 1] = make_float4(hi[0][1], hi[0][2], lo[1][0], lo[1][1]);
+        node[4 * o + 2] = make_float4(lo[1][2], hi[1][0], hi[1][1], hi[1][2]);
+        node[4 * o + 3] = make_float4(__int_as_float(ref[0]), __int_as_float(ref[1]), 0.0f, 0.0f);
+    }
+}
+
+template <int D>
+__global__ void k_leaf_data(const unsigned long long *keys, int n, const float4 *seg, const float *seginv,
+                            const float4 *tri, float4 *lseg, float *lseginv, float4 *ltri, int *lorig) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int f = (int)(unsigned)keys[s];
+    lorig[s] = f;
+    if (D == 2) {
+        lseg[s] = seg[f];
+        lseginv[s] = seginv[f];
+    } else {
+        ltri[3 * s] = tri[3 * f];
+        ltri[3 * s + 1] = tri[3 * f + 1];
+        ltri[3 * s + 2] = tri[3 * f + 2];
+    }
+}
+
+// ------------------------------------------------------------------ host
+static inline int nblk(long long n, int b) { return (int)((n + b - 1) / b); }
+
+template <typename T>
+static cudaError_t dalloc(T **p, size_t count, cudaStream_t st) {
+    if (count == 0) count = 1;
+    return cudaMallocAsync((void **)p, count * sizeof(T), st);
+}
+
+void SceneImpl::release(cudaStream_t st) {
+    void *ptrs[] = {V, F, N, g, seg, seginv, tri, node, lseg, lseginv, ltri, lorig, cdf};
+    for (void *p : ptrs)
+        if (p) cudaFreeAsync(p, st);
+    V = nullptr;
+    F = nullptr;
+    N = nullptr;
+    g = nullptr;
+    seg = nullptr;
+    seginv = nullptr;
+    tri = nullptr;
+    node = nullptr;
+    lseg = nullptr;
+    lseginv = nullptr;
+    ltri = nullptr;
+    lorig = nullptr;
+    cdf = nullptr;
+}
+
+// Normalised CDF of pmf_i ~ r_i log(1/r_i), r_i = (i + 0.5)/n, built in
+// double on the host (include/tabulated_G_cdf.cuh:5-8 regenerated from its
+// formula, wos/wos_with_source.py:17-23).
+void build_g_cdf(std::vector<float> &cdf, int n) {
+    std::vector<double> pmf(n);
+    double total = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const double r = (i + 0.5) / n;
+        pmf[i] = r * std::log(1.0 / r) / (2.0 * 3.14159265358979323846);
+        total += pmf[i];
+    }
+    cdf.resize(n);
+    double acc = 0.0;
+    for (int i = 0; i < n; ++i) {
+        acc += pmf[i];
+        cdf[i] = (float)(acc / total);
+    }
+    cdf[n - 1] = 1.0f;
+}
+
+template <int D>
+static int build_geometry(SceneImpl &S, cudaStream_t st) {
+    const int nV = S.nV, nF = S.nF;
+    const int TB = 256;
+    // ---- AABB
+    int *lohi = nullptr;
+    WOS_TRY(dalloc(&lohi, 6, st));
+    {
+        int init[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, (int)0x80000000, (int)0x80000000, (int)0x80000000};
+        WOS_TRY(cudaMemcpyAsync(lohi, init, sizeof(init), cudaMemcpyHostToDevice, st));
+        WOS_TRY(cudaStreamSynchronize(st));
+    }
+    k_aabb<<<std::min(nblk(nV, TB), 1024), TB, 0, st>>>(S.V, nV, D, lohi);
+    int lohi_h[6];
+    WOS_TRY(cudaMemcpyAsync(lohi_h, lohi, sizeof(lohi_h), cudaMemcpyDeviceToHost, st));
+    WOS_TRY(cudaStreamSynchronize(st));
+    cudaFreeAsync(lohi, st);
+    auto from_ord = [](int i) {
+        int b = i >= 0 ? i : i ^ 0x7fffffff;
+        float f;
+        memcpy(&f, &b, 4);
+        return f;
+    };
+    for (int k = 0; k < 3; ++k) {
+        S.lo[k] = k < D ? from_ord(lohi_h[k]) : 0.0f;
+        S.hi[k] = k < D ? from_ord(lohi_h[3 + k]) : 0.0f;
+    }
+    float ext = INFINITY;
+    for (int k = 0; k < D; ++k) ext = fminf(ext, fabsf(S.hi[k] - S.lo[k]));
+    S.half_min_extent = ext * 0.5f;
+
+    // ---- vertex normals
+    {
+        const int ns = nF * D;
+        float *contrib = nullptr;
+        unsigned long long *keys = nullptr, *keys2 = nullptr;
+        int *beg = nullptr, *end = nullptr;
+        WOS_TRY(dalloc(&contrib, (size_t)ns * D, st));
+        WOS_TRY(dalloc(&keys, ns, st));
+        WOS_TRY(dalloc(&keys2, ns, st));
+        WOS_TRY(dalloc(&beg, nV, st));
+        WOS_TRY(dalloc(&end, nV, st));
+        WOS_TRY(cudaMemsetAsync(beg, 0, sizeof(int) * nV, st));
+        WOS_TRY(cudaMemsetAsync(end, 0, sizeof(int) * nV, st));
+        k_face_normals<D><<<nblk(nF, TB), TB, 0, st>>>(S.V, S.F, nF, contrib, keys);
+        size_t tmp_bytes = 0;
+        cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, keys, keys2, ns, 0, 64, st);
+        void *tmp = nullptr;
+        WOS_TRY(cudaMallocAsync(&tmp, tmp_bytes, st));
+        WOS_TRY(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, keys, keys2, ns, 0, 64, st));
+        k_segments<<<nblk(ns, TB), TB, 0, st>>>(keys2, ns, beg, end);
+        k_vertex_normals<D><<<nblk(nV, TB), TB, 0, st>>>(keys2, contrib, beg, end, nV, S.N);
+        WOS_TRY(cudaGetLastError());
+        cudaFreeAsync(tmp, st);
+        cudaFreeAsync(contrib, st);
+        cudaFreeAsync(keys, st);
+        cudaFreeAsync(keys2, st);
+        cudaFreeAsync(beg, st);
+        cudaFreeAsync(end, st);
+    }
+
+    // ---- primitives + Morton keys
+    float *pbox = nullptr;
+    unsigned long long *mkeys = nullptr, *skeys = nullptr;
+    WOS_TRY(dalloc(&pbox, (size_t)nF * 2 * D, st));
+    WOS_TRY(dalloc(&mkeys, nF, st));
+    WOS_TRY(dalloc(&skeys, nF, st));
+    k_prims<D><<<nblk(nF, TB), TB, 0, st>>>(S.V, S.F, nF, S.lo[0], S.lo[1], S.lo[2], S.hi[0], S.hi[1], S.hi[2], S.seg,
+                                           S.seginv, S.tri, pbox, mkeys);
+    {
+        size_t tmp_bytes = 0;
+        cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, mkeys, skeys, nF, 0, 64, st);
+        void *tmp = nullptr;
+        WOS_TRY(cudaMallocAsync(&tmp, tmp_bytes, st));
+        WOS_TRY(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, mkeys, skeys, nF, 0, 64, st));
+        cudaFreeAsync(tmp, st);
+    }
+    k_leaf_data<D><<<nblk(nF, TB), TB, 0, st>>>(skeys, nF, S.seg, S.seginv, S.tri, S.lseg, S.lseginv, S.ltri, S.lorig);
+
+    // ---- hierarchy
+    const int nInt = nF - 1;
+    S.nNodes = nInt;
+    S.depth = 0;
+    if (nInt > 0) {
+        int2 *child = nullptr;
+        int *pint = nullptr, *pleaf = nullptr, *flags = nullptr, *maxd = nullptr, *new_of_old = nullptr;
+        float *nbox = nullptr;
+        unsigned long long *dkeys = nullptr, *dkeys2 = nullptr;
+        WOS_TRY(dalloc(&child, nInt, st));
+        WOS_TRY(dalloc(&pint, nInt, st));
+        WOS_TRY(dalloc(&pleaf, nF, st));
+        WOS_TRY(dalloc(&flags, nInt, st));
+        WOS_TRY(dalloc(&maxd, 1, st));
+        WOS_TRY(dalloc(&new_of_old, nInt, st));
+        WOS_TRY(dalloc(&nbox, (size_t)nInt * 2 * D, st));
+        WOS_TRY(dalloc(&dkeys, nInt, st));
+        WOS_TRY(dalloc(&dkeys2, nInt, st));
+        WOS_TRY(cudaMemsetAsync(pint, 0xff, sizeof(int) * nInt, st));
+        WOS_TRY(cudaMemsetAsync(pleaf, 0xff, sizeof(int) * nF, st));
+        WOS_TRY(cudaMemsetAsync(flags, 0, sizeof(int) * nInt, st));
+        WOS_TRY(cudaMemsetAsync(maxd, 0, sizeof(int), st));
+        k_karras<<<nblk(nInt, TB), TB, 0, st>>>(skeys, nF, child, pint, pleaf);
+        k_refit<D><<<nblk(nF, TB), TB, 0, st>>>(skeys, nF, pbox, child, pint, pleaf, flags, nbox);
+        k_depth<<<nblk(nInt, TB), TB, 0, st>>>(pint, nInt, dkeys, maxd);
+        size_t tmp_bytes = 0;
+        cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, dkeys, dkeys2, nInt, 0, 64, st);
+        void *tmp = nullptr;
+        WOS_TRY(cudaMallocAsync(&tmp, tmp_bytes, st));
+        WOS_TRY(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, dkeys, dkeys2, nInt, 0, 64, st));
+        k_bfs_rank<<<nblk(nInt, TB), TB, 0, st>>>(dkeys2, nInt, new_of_old);
+        k_write_nodes<D><<<nblk(nInt, TB), TB, 0, st>>>(skeys, nInt, pbox, nbox, child, new_of_old, S.node);
+        WOS_TRY(cudaGetLastError());
+        int maxd_h = 0;
+        WOS_TRY(cudaMemcpyAsync(&maxd_h, maxd, sizeof(int), cudaMemcpyDeviceToHost, st));
+        WOS_TRY(cudaStreamSynchronize(st));
+        S.depth = maxd_h;
+        cudaFreeAsync(tmp, st);
+        cudaFreeAsync(child, st);
+        cudaFreeAsync(pint, st);
+        cudaFreeAsync(pleaf, st);
+        cudaFreeAsync(flags, st);
+        cudaFreeAsync(maxd, st);
+        cudaFreeAsync(new_of_old, st);
+        cudaFreeAsync(nbox, st);
+        cudaFreeAsync(dkeys, st);
+        cudaFreeAsync(dkeys2, st);
+    }
+    cudaFreeAsync(pbox, st);
+    cudaFreeAsync(mkeys, st);
+    cudaFreeAsync(skeys, st);
+    WOS_TRY(cudaGetLastError());
+    WOS_TRY(cudaStreamSynchronize(st));
+    return 0;
+}
+
+int SceneImpl::allocate(cudaStream_t st) {
+    const int D = dim;
+    WOS_TRY(dalloc(&V, (size_t)nV * D, st));
+    WOS_TRY(dalloc(&F, (size_t)nF * D, st));
+    WOS_TRY(dalloc(&N, (size_t)nV * D, st));
+    WOS_TRY(dalloc(&g, nV, st));
+    if (D == 2) {
+        WOS_TRY(dalloc(&seg, nF, st));
+        WOS_TRY(dalloc(&seginv, nF, st));
+        WOS_TRY(dalloc(&lseg, nF, st));
+        WOS_TRY(dalloc(&lseginv, nF, st));
+        WOS_TRY(dalloc(&node, (size_t)std::max(nF - 1, 1) * 3, st));
+    } else {
+        WOS_TRY(dalloc(&tri, (size_t)nF * 3, st));
+        WOS_TRY(dalloc(&ltri, (size_t)nF * 3, st));
+        WOS_TRY(dalloc(&node, (size_t)std::max(nF - 1, 1) * 4, st));
+    }
+    WOS_TRY(dalloc(&lorig, nF, st));
+    std::vector<float> c;
+    build_g_cdf(c, 10000);
+    n_cdf = (int)c.size();
+    WOS_TRY(dalloc(&cdf, c.size(), st));
+    WOS_TRY(cudaMemcpyAsync(cdf, c.data(), c.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    WOS_TRY(cudaStreamSynchronize(st));
+    return 0;
+}
+
+int SceneImpl::check_indices(cudaStream_t st) {
+    int *bad = nullptr;
+    WOS_TRY(dalloc(&bad, 1, st));
+    WOS_TRY(cudaMemsetAsync(bad, 0, sizeof(int), st));
+    const long long n = (long long)nF * dim;
+    k_check_indices<<<std::min(nblk(n, 256), 4096), 256, 0, st>>>(F, n, nV, bad);
+    int bad_h = 0;
+    WOS_TRY(cudaMemcpyAsync(&bad_h, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+    WOS_TRY(cudaStreamSynchronize(st));
+    cudaFreeAsync(bad, st);
+    if (bad_h) return fail(WOS_ERR_INVALID_ARGUMENT, "face index out of range [0, nV)");
+    return 0;
+}
+
+int SceneImpl::build(cudaStream_t st) { return dim == 2 ? build_geometry<2>(*this, st) : build_geometry<3>(*this, st); }
+
+SceneView SceneImpl::view() const {
+    SceneView v{};
+    v.dim = dim;
+    v.nV = nV;
+    v.nF = nF;
+    v.V = V;
+    v.F = F;
+    v.N = N;
+    v.g = g;
+    v.seg = seg;
+    v.seginv = seginv;
+    v.tri = tri;
+    v.nNodes = nNodes;
+    v.node = node;
+    v.lseg = lseg;
+    v.lseginv = lseginv;
+    v.ltri = ltri;
+    v.lorig = lorig;
+    for (int k = 0; k < 3; ++k) {
+        v.lo[k] = lo[k];
+        v.hi[k] = hi[k];
+    }
+    v.half_min_extent = half_min_extent;
+    v.src_type = src_type;
+    for (int k = 0; k < 5; ++k) v.src[k] = src[k];
+    v.cdf = cdf;
+    v.n_cdf = n_cdf;
+    return v;
+}
+
+}  // namespace wosd

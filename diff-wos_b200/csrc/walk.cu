@@ -1,0 +1,957 @@
+// Walk-on-spheres kernels for sm_100a.
+//
+// Forward: a persistent kernel in which every warp keeps 32 walks in flight.
+// Each loop iteration runs exactly one nearest-primitive query per lane;
+// when a lane's walk ends, the warp refills idle lanes from a grabbed chunk
+// of the flattened (point, walk) index space (ballot + prefix rank), so
+// warps stay full while walk lengths differ.  Results depend only on the
+// Philox counters, never on which lane or block ran a walk.
+//
+// Adjoint: the same persistent loop over (point, walk) samples, each sample a
+// small state machine -- primal walk, 10-step inscribed-ball bisection, two
+// antithetic walks on the ball -- in which every state transition is again one
+// nearest query, so lanes in different phases share the query code path.
+//
+// Reference functions restated: WoSDevice<N>::walk (include/wos.cuh:97-145),
+// WoS<N>::solve / singleWalk launchers (:184-448), normal_derivative
+// (wos/wos.py:184-232, wos/wos_with_source.py:154-232, wos/wos3d.py:248-286),
+// tangent_derivative (wos/scene.py:451-460, wos/wos3d.py:288-307), OursCUDA /
+// Ours3D (wos/wos_grad.py:130-151, wos/wos_grad_3d.py:391-411).
+#include <algorithm>
+
+#include "scene_impl.h"
+#include "walk.h"
+
+namespace wosd {
+
+__device__ int g_status;
+
+int read_status(int reset, int *out) {
+    int v = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&v, g_status, sizeof(int));
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpyFromSymbol(g_status)");
+    if (reset) {
+        const int z = 0;
+        e = cudaMemcpyToSymbol(g_status, &z, sizeof(int));
+        if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpyToSymbol(g_status)");
+    }
+    *out = v;
+    return 0;
+}
+
+template <int D, bool BVH>
+__device__ __forceinline__ Hit query(const SceneView &S, const float *p, const float4 *top, int n_top) {
+    if (BVH) return nearest_bvh<D>(S, p, top, n_top, &g_status);
+    return nearest_brute<D>(S, p);
+}
+
+// ------------------------------------------------------------------ walker
+enum { W_CONTINUE = 0, W_VALID = 1, W_INVALID = 2, W_TRUNC = 3 };
+
+struct Walker {
+    float p[3];
+    float contrib;
+    float ds[5];
+    int i;
+    bool fresh;
+    __device__ __forceinline__ void start(const float *x, int D) {
+        p[0] = x[0];
+        p[1] = x[1];
+        p[2] = D == 3 ? x[2] : 0.0f;
+        contrib = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) ds[k] = 0.0f;
+        i = 0;
+        fresh = true;
+    }
+};
+
+// Process the query result at w.p: inside test on the first query, shell
+// test, truncation, then the source term and one step (include/wos.cuh:97-145).
+template <int D>
+__device__ __forceinline__ int walker_advance(Walker &w, const SceneView &S, const Hit &hit, const WalkCfg &c,
+                                              float eps, bool project, bool prevent_fd, uint32_t pt, uint32_t wk,
+                                              uint32_t role, bool want_ds, const float *cdf) {
+    float d = sqrtf(hit.d2);
+    if (w.fresh) {
+        w.fresh = false;
+        if (!c.double_sided && !inside_test<D>(S, w.p, hit, nullptr)) return W_INVALID;
+        if (prevent_fd) d *= 0.5f;
+    }
+    if (w.i < c.nsteps) {
+        if (d < eps) return W_VALID;
+        if (!project && w.i == c.nsteps - 1) return W_TRUNC;
+        const uint4 r = philox(c.rng, pt, wk, (uint32_t)w.i, role);
+        if (D == 2 && S.src_type != 0) {
+            float yx, yy;
+            const float K = source_step(S, cdf, c.use_IS != 0, w.p[0], w.p[1], d, r.z, r.w, yx, yy);
+            float df[5];
+            const float f = source(S, yx, yy, want_ds ? df : nullptr);
+            w.contrib = fmaf(f, K, w.contrib);
+            if (want_ds) {
+#pragma unroll
+                for (int k = 0; k < 5; ++k) w.ds[k] = fmaf(df[k], K, w.ds[k]);
+            }
+        }
+        if (D == 2) {
+            float s, cs;
+            wosm::sincos_2pi(wosm::u01(r.x), &s, &cs);
+            w.p[0] = fmaf(cs, d, w.p[0]);
+            w.p[1] = fmaf(s, d, w.p[1]);
+        } else {
+            const float z = fmaf(-2.0f, wosm::u01(r.x), 1.0f);
+            const float rr = sqrtf(fmaxf(0.0f, fmaf(-z, z, 1.0f)));
+            float s, cs;
+            wosm::sincos_2pi(wosm::u01(r.y), &s, &cs);
+            w.p[0] = fmaf(rr * cs, d, w.p[0]);
+            w.p[1] = fmaf(rr * s, d, w.p[1]);
+            w.p[2] = fmaf(z, d, w.p[2]);
+        }
+        w.i += 1;
+        return W_CONTINUE;
+    }
+    return project ? W_VALID : W_TRUNC;
+}
+
+// Stage the shallowest LBVH nodes and (optionally) the G CDF in shared memory.
+template <int D, bool BVH>
+__device__ __forceinline__ void stage_smem(const SceneView &S, int n_top, bool stage_cdf, float4 *smem,
+                                           const float4 *&top, const float *&cdf) {
+    constexpr int K = NodeWords<D>::K;
+    const int nt = BVH ? n_top : 0;
+    for (int t = threadIdx.x; t < nt * K; t += blockDim.x) smem[t] = S.node[t];
+    float *scdf = reinterpret_cast<float *>(smem + nt * K);
+    cdf = S.cdf;
+    if (stage_cdf) {
+        for (int t = threadIdx.x; t < S.n_cdf; t += blockDim.x) scdf[t] = S.cdf[t];
+        cdf = scdf;
+    }
+    top = smem;
+    __syncthreads();
+}
+
+// Warp-uniform refill of idle lanes from chunks of the global index space.
+// Returns false once the warp has no work left.
+struct Queue {
+    long long cb, ce;
+    bool drained;
+};
+
+__device__ __forceinline__ bool refill(Queue &q, bool &active, long long &idx, unsigned long long *counter,
+                                       long long total, int chunk) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    unsigned idle = __ballot_sync(FULL, !active);
+    bool got = false;
+    while (idle != 0u && !q.drained) {
+        if (q.cb >= q.ce) {
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(counter, (unsigned long long)chunk);
+            base = __shfl_sync(FULL, base, 0);
+            if ((long long)base >= total) {
+                q.drained = true;
+                break;
+            }
+            q.cb = (long long)base;
+            q.ce = min((long long)base + chunk, total);
+        }
+        const int nidle = __popc(idle);
+        const long long avail = min((long long)nidle, q.ce - q.cb);
+        const int rank = __popc(idle & ((1u << lane) - 1u));
+        if (!active && rank < avail) {
+            idx = q.cb + rank;
+            active = true;
+            got = true;
+        }
+        q.cb += avail;
+        idle = __ballot_sync(FULL, !active);
+    }
+    (void)got;
+    return __ballot_sync(FULL, active) != 0u;
+}
+
+// ------------------------------------------------------------------ forward
+template <int D, bool BVH, bool RECORDS>
+__global__ void __launch_bounds__(512) k_walk(SceneView S, WalkCfg c, const float *__restrict__ P, long long total,
+                                             unsigned long long *counter, int chunk, int n_top, int stage_cdf,
+                                             WalkOut out) {
+    extern __shared__ float4 smem[];
+    const float4 *top;
+    const float *cdf;
+    stage_smem<D, BVH>(S, n_top, stage_cdf != 0, smem, top, cdf);
+    Queue q{0, 0, false};
+    bool active = false;
+    long long idx = 0;
+    uint32_t pt = 0, wk = 0;
+    Walker w;
+    for (;;) {
+        const bool was = active;
+        if (!refill(q, active, idx, counter, total, chunk)) break;
+        if (active && !was) {
+            if (RECORDS) {
+                pt = (uint32_t)idx;
+                wk = c.walk_offset;
+            } else {
+                pt = (uint32_t)(idx / c.nwalks);
+                wk = c.walk_offset + (uint32_t)(idx - (long long)pt * c.nwalks);
+            }
+            w.start(P + (size_t)pt * D, D);
+        }
+        if (!active) continue;
+        const Hit hit = query<D, BVH>(S, w.p, top, n_top);
+        const int r = walker_advance<D>(w, S, hit, c, c.eps, c.project != 0, c.prevent_fd != 0, pt, wk, ROLE_PRIMAL,
+                                        false, cdf);
+        if (r == W_CONTINUE) continue;
+        active = false;
+        if (RECORDS) {
+            const bool ok = r == W_VALID;
+            out.valid[pt] = ok ? 1 : 0;
+            Rec rec;
+            if (ok) rec = closest_record<D>(S, w.p, hit.prim);
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                if (out.pt) out.pt[(size_t)pt * D + k] = ok ? rec.p[k] : 0.0f;
+                if (out.nrm) out.nrm[(size_t)pt * D + k] = ok ? rec.n[k] : 0.0f;
+            }
+            if (out.tuv) {
+                out.tuv[2 * (size_t)pt] = ok ? rec.t0 : 0.0f;
+                out.tuv[2 * (size_t)pt + 1] = (ok && D == 3) ? rec.t1 : 0.0f;
+            }
+            if (out.prim) out.prim[pt] = ok ? hit.prim : -1;
+            if (out.contrib) out.contrib[pt] = ok ? w.contrib : 0.0f;
+        } else {
+            float v = 0.0f;
+            if (r == W_VALID) {
+                const Rec rec = closest_record<D>(S, w.p, hit.prim);
+                v = dirichlet<D>(S, hit.prim, rec.t0, rec.t1, nullptr, nullptr);
+                if (c.include_source) v += w.contrib;
+                if (!isfinite(v)) atomicOr(&g_status, ST_NONFINITE);
+            }
+            out.values[idx] = v;
+            if (out.steps) out.steps[idx] = r == W_TRUNC ? c.nsteps : w.i;
+        }
+    }
+}
+
+// Reference-shaped kernel: one thread per (point, walk), no regeneration.
+template <int D, bool BVH>
+__global__ void __launch_bounds__(256) k_walk_plain(SceneView S, WalkCfg c, const float *__restrict__ P,
+                                                   long long total, float *values) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const uint32_t pt = (uint32_t)(idx / c.nwalks);
+    const uint32_t wk = c.walk_offset + (uint32_t)(idx - (long long)pt * c.nwalks);
+    Walker w;
+    w.start(P + (size_t)pt * D, D);
+    float v = 0.0f;
+    for (;;) {
+        const Hit hit = query<D, BVH>(S, w.p, nullptr, 0);
+        const int r = walker_advance<D>(w, S, hit, c, c.eps, c.project != 0, c.prevent_fd != 0, pt, wk, ROLE_PRIMAL,
+                                        false, S.cdf);
+        if (r == W_CONTINUE) continue;
+        if (r == W_VALID) {
+            const Rec rec = closest_record<D>(S, w.p, hit.prim);
+            v = dirichlet<D>(S, hit.prim, rec.t0, rec.t1, nullptr, nullptr);
+            if (c.include_source) v += w.contrib;
+        }
+        break;
+    }
+    values[idx] = v;
+}
+
+// Per-point FP64 mean and sample variance, one warp per point, Neumaier
+// compensated partial sums combined across lanes.
+__device__ __forceinline__ void neumaier_add(double &s, double &c, double x) {
+    const double t = s + x;
+    c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+    s = t;
+}
+
+__device__ __forceinline__ double warp_sum_comp(double s, double c) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double s2 = __shfl_down_sync(0xffffffffu, s, o);
+        const double c2 = __shfl_down_sync(0xffffffffu, c, o);
+        c += c2;
+        neumaier_add(s, c, s2);
+    }
+    return __shfl_sync(0xffffffffu, s + c, 0);
+}
+
+__global__ void k_reduce(const float *__restrict__ vals, int n, int nw, double *mean, double *var) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const float *v = vals + (size_t)warp * nw;
+    double s = 0.0, cc = 0.0;
+    for (int w = lane; w < nw; w += 32) neumaier_add(s, cc, (double)v[w]);
+    const double m = warp_sum_comp(s, cc) / nw;
+    if (var) {
+        double q = 0.0, qc = 0.0;
+        for (int w = lane; w < nw; w += 32) {
+            const double e = (double)v[w] - m;
+            neumaier_add(q, qc, e * e);
+        }
+        const double qq = warp_sum_comp(q, qc);
+        if (lane == 0) var[warp] = nw > 1 ? qq / (nw - 1) : 0.0;
+    }
+    if (lane == 0) mean[warp] = m;
+}
+
+// ------------------------------------------------------------------ queries
+template <int D, bool BVH>
+__global__ void k_closest(SceneView S, const float *__restrict__ P, int n, QueryOut o) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float p[3] = {P[(size_t)i * D], P[(size_t)i * D + 1], D == 3 ? P[(size_t)i * D + 2] : 0.0f};
+    const Hit hit = query<D, BVH>(S, p, nullptr, 0);
+    if (o.prim) o.prim[i] = hit.prim;
+    if (o.dist) o.dist[i] = sqrtf(hit.d2);
+    if (hit.prim < 0) {
+        atomicOr(&g_status, ST_BAD_PRIM);
+        return;
+    }
+    const Rec r = closest_record<D>(S, p, hit.prim);
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        if (o.pt) o.pt[(size_t)i * D + k] = r.p[k];
+        if (o.nrm) o.nrm[(size_t)i * D + k] = r.n[k];
+    }
+    if (o.tuv) {
+        o.tuv[2 * (size_t)i] = r.t0;
+        o.tuv[2 * (size_t)i + 1] = D == 3 ? r.t1 : 0.0f;
+    }
+    if (o.sdf || o.inside) {
+        float sd;
+        const bool in = inside_test<D>(S, p, hit, &sd);
+        if (o.sdf) o.sdf[i] = sd;
+        if (o.inside) o.inside[i] = in ? 1 : 0;
+    }
+}
+
+// Largest inscribed ball (include/scene.cuh:225-249).
+template <int D, bool BVH>
+__device__ __forceinline__ float inscribed_ball(const SceneView &S, const float *p, const float *n, float eps,
+                                                const float4 *top, int n_top) {
+    float b = S.half_min_extent, a = eps;
+    for (int i = 0; i < 10; ++i) {
+        const float m = (a + b) * 0.5f;
+        float q[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int k = 0; k < D; ++k) q[k] = fmaf(n[k], m, p[k]);
+        const float d = sqrtf(query<D, BVH>(S, q, top, n_top).d2);
+        if (fabsf(d - m) < 1e-5f)
+            a = m;
+        else
+            b = m;
+    }
+    return a;
+}
+
+template <int D, bool BVH>
+__global__ void k_ball(SceneView S, const uint8_t *valid, const float *pt, const float *nrm, int n, float eps,
+                       float *R) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (!valid[i]) {
+        R[i] = 0.0f;
+        return;
+    }
+    float p[3] = {0, 0, 0}, nn[3] = {0, 0, 0};
+    for (int k = 0; k < D; ++k) {
+        p[k] = pt[(size_t)i * D + k];
+        nn[k] = nrm[(size_t)i * D + k];
+    }
+    R[i] = inscribed_ball<D, BVH>(S, p, nn, eps, nullptr, 0);
+}
+
+// ------------------------------------------------------------------ adjoint
+template <int D>
+__device__ __forceinline__ void tangent_derivative(const SceneView &S, int prim, float *out) {
+    if (D == 2) {
+        const float4 s = __ldg(&S.seg[prim]);
+        const int ia = __ldg(&S.F[2 * prim]), ib = __ldg(&S.F[2 * prim + 1]);
+        const float len = sqrtf(dot2(s.z, s.w, s.z, s.w));
+        const float dv = (__ldg(&S.g[ib]) - __ldg(&S.g[ia])) / len;
+        out[0] = dv * (s.z / len);
+        out[1] = dv * (s.w / len);
+    } else {
+        const float4 t1 = __ldg(&S.tri[3 * prim + 1]), t2 = __ldg(&S.tri[3 * prim + 2]);
+        const int ia = __ldg(&S.F[3 * prim]), ib = __ldg(&S.F[3 * prim + 1]), ic = __ldg(&S.F[3 * prim + 2]);
+        const float ab[3] = {t1.x, t1.y, t1.z}, ac[3] = {t2.x, t2.y, t2.z};
+        const float lab = sqrtf(dot3(ab[0], ab[1], ab[2], ab[0], ab[1], ab[2]));
+        float t[3], fn[3], n[3];
+        for (int k = 0; k < 3; ++k) t[k] = ab[k] / lab;
+        cross3(ab[0], ab[1], ab[2], ac[0], ac[1], ac[2], fn[0], fn[1], fn[2]);
+        const float lfn = sqrtf(dot3(fn[0], fn[1], fn[2], fn[0], fn[1], fn[2]));
+        for (int k = 0; k < 3; ++k) fn[k] = fn[k] / lfn;
+        cross3(fn[0], fn[1], fn[2], t[0], t[1], t[2], n[0], n[1], n[2]);
+        const float ln = sqrtf(dot3(n[0], n[1], n[2], n[0], n[1], n[2]));
+        for (int k = 0; k < 3; ++k) n[k] = n[k] / ln;
+        const float va = __ldg(&S.g[ia]), vb = __ldg(&S.g[ib]), vc = __ldg(&S.g[ic]);
+        const float gt = (vb - va) / lab;
+        const float gn = ((vc - va) - gt * dot3(ac[0], ac[1], ac[2], t[0], t[1], t[2])) /
+                         dot3(ac[0], ac[1], ac[2], n[0], n[1], n[2]);
+        for (int k = 0; k < 3; ++k) out[k] = fmaf(gt, t[k], gn * n[k]);
+    }
+}
+
+__device__ __forceinline__ float eval_P(const float *c, const float *y, const float *s, float R) {
+    const float yy0 = y[0] - c[0], yy1 = y[1] - c[1];
+    const float ss0 = s[0] - c[0], ss1 = s[1] - c[1];
+    const float rr = dot2(yy0, yy1, yy0, yy1);
+    const float cc = dot2(yy0, yy1, ss0, ss1) / sqrtf(dot2(ss0, ss1, ss0, ss1));
+    const float RR = R * R;
+    const float denom = fmaf(-2.0f * R, cc, RR) + rr;
+    return (RR - rr) / fmaxf(denom, 1e-5f) / (wosm::kTwoPi * R);
+}
+
+// State of one normal-derivative sample on the inscribed ball of radius R
+// centred at c (wos/wos.py:196-232, wos/wos3d.py:254-286).
+struct NdState {
+    float n[3];    // outward normal (-record normal)
+    float p[3];    // boundary point
+    float c[3];    // ball centre
+    float R;
+    float uref;
+    float cs, sn;  // 2D: cos/sin theta.  3D: cos theta, sqrt(1 - cos^2)
+    float cph, sph;
+    float pd[3], pd2[3];
+    float gsum;
+    int which;
+};
+
+template <int D>
+__device__ __forceinline__ void nd_setup(NdState &st, const SceneView &S, const WalkCfg &c, const AdjCfg &a,
+                                         uint32_t pt, uint32_t wk) {
+    const uint4 rx = philox(c.rng, pt, wk, 0, ROLE_EXTRA);
+#pragma unroll
+    for (int k = 0; k < D; ++k) st.c[k] = fmaf(-st.n[k], st.R, st.p[k]);
+    if (D == 2) {
+        const float cu = a.clamping * wosm::kInv2Pi;
+        const float u = fminf(fmaxf(wosm::u01(rx.x), cu), 1.0f - cu);
+        wosm::sincos_2pi(u, &st.sn, &st.cs);
+        st.pd[0] = -st.n[1];
+        st.pd[1] = st.n[0];
+    } else {
+        st.cs = fminf(fmaxf(fmaf(-2.0f, wosm::u01(rx.x), 1.0f), -1.0f), 1.0f - a.clamping);
+        wosm::sincos_2pi(wosm::u01(rx.y), &st.sph, &st.cph);
+        const bool zu = fabsf(st.n[2]) < 0.9f;
+        const float up0 = zu ? 0.0f : 1.0f, up2 = zu ? 1.0f : 0.0f;
+        cross3(st.n[0], st.n[1], st.n[2], up0, 0.0f, up2, st.pd[0], st.pd[1], st.pd[2]);
+        const float l = sqrtf(dot3(st.pd[0], st.pd[1], st.pd[2], st.pd[0], st.pd[1], st.pd[2]));
+        for (int k = 0; k < 3; ++k) st.pd[k] = st.pd[k] / l;
+        cross3(st.n[0], st.n[1], st.n[2], st.pd[0], st.pd[1], st.pd[2], st.pd2[0], st.pd2[1], st.pd2[2]);
+        st.sn = sqrtf(fmaxf(0.0f, fmaf(-st.cs, st.cs, 1.0f)));
+    }
+    st.gsum = 0.0f;
+    st.which = 0;
+}
+
+// Query point of antithetic sample st.which.
+template <int D>
+__device__ __forceinline__ void nd_point(const NdState &st, float *q) {
+    if (D == 2) {
+        const float si = st.which == 0 ? st.sn : -st.sn;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) q[k] = fmaf(st.R, fmaf(st.n[k], st.cs, st.pd[k] * si), st.c[k]);
+        q[2] = 0.0f;
+    } else {
+        const float cp = st.which == 0 ? st.cph : -st.cph, sp = st.which == 0 ? st.sph : -st.sph;
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            q[k] = fmaf(st.R, fmaf(st.cs, st.n[k], st.sn * fmaf(cp, st.pd[k], sp * st.pd2[k])), st.c[k]);
+    }
+}
+
+template <int D>
+__device__ __forceinline__ void nd_accumulate(NdState &st, const AdjCfg &a, float uq) {
+    float P;
+    if (D == 2) {
+        P = 1.0f / (st.cs - 1.0f);
+    } else {
+        const float om = 1.0f - st.cs;
+        P = -1.0f / (1.41421356f * (om * sqrtf(om)));
+    }
+    st.gsum += a.control_variates ? P * (uq - st.uref) / st.R : P * uq / st.R;
+}
+
+// grad * n_out, including the 2D interior source term.
+template <int D>
+__device__ __forceinline__ void nd_finish(const NdState &st, const SceneView &S, const WalkCfg &c, const AdjCfg &a,
+                                          uint32_t pt, uint32_t wk, bool with_src, float *out) {
+    float grad = st.gsum * 0.5f;
+    if (D == 2 && with_src) {
+        const uint4 rx = philox(c.rng, pt, wk, 0, ROLE_EXTRA);
+        float ds, dc;
+        wosm::sincos_2pi(wosm::u01(rx.w), &ds, &dc);
+        const float rr = sqrtf(wosm::u01(rx.z));
+        const float y[2] = {fmaf(st.R, rr * dc, st.c[0]), fmaf(st.R, rr * ds, st.c[1])};
+        const float f = source(S, y[0], y[1], nullptr);
+        const float P = eval_P(st.c, y, st.p, st.R);
+        const float area = wosm::kPi * st.R * st.R;
+        float ci;
+        if (a.control_variates) {
+            const float fs = source(S, st.p[0], st.p[1], nullptr);
+            ci = (f - fs) * P * area + fs * st.R * 0.5f;
+        } else {
+            ci = f * P * area;
+        }
+        grad = grad - ci;
+    }
+#pragma unroll
+    for (int k = 0; k < D; ++k) out[k] = grad * st.n[k];
+}
+
+enum { PH_IDLE = 0, PH_PRIMAL = 1, PH_BALL = 2, PH_ANTI_START = 3, PH_ANTI_WALK = 4, PH_ND_START = 5 };
+
+// Persistent adjoint kernel.  ND_ONLY: the items are boundary records and the
+// kernel writes one normal-derivative estimate per record (the
+// wos_normal_derivative entry point); otherwise items are (point, walk)
+// samples and gradients are accumulated into dV / dg / dsrc.
+template <int D, bool BVH, bool ND_ONLY>
+__global__ void __launch_bounds__(512) k_adjoint(SceneView S, WalkCfg c, AdjCfg a, const float *__restrict__ P,
+                                                long long total, const float *__restrict__ dLdu,
+                                                unsigned long long *counter, int chunk, int n_top, int stage_cdf,
+                                                AdjOut out) {
+    extern __shared__ float4 smem[];
+    const float4 *top;
+    const float *cdf;
+    stage_smem<D, BVH>(S, n_top, stage_cdf != 0, smem, top, cdf);
+    const bool src2 = D == 2 && S.src_type != 0;
+    const bool want_src = !ND_ONLY && a.want_dsrc && c.include_source && src2;
+    const bool with_src = a.source_in_nd && src2;
+    Queue q{0, 0, false};
+    bool active = false;
+    long long idx = 0;
+    uint32_t pt = 0, wk = 0;
+    int phase = PH_IDLE;
+    double W = 0.0;
+    Walker w;
+    NdState st;
+    int rprim = 0;
+    float rt0 = 0.0f, rt1 = 0.0f;
+    float rn[3] = {0, 0, 0};
+    float qpos[3] = {0, 0, 0};
+    float ba = 0.0f, bb = 0.0f;
+    int bk = 0;
+    double acc_src[5] = {0, 0, 0, 0, 0};
+
+    for (;;) {
+        const bool was = active;
+        if (!refill(q, active, idx, counter, total, chunk)) break;
+        if (active && !was) {
+            if (ND_ONLY) {
+                pt = (uint32_t)idx;
+                wk = c.walk_offset;
+                if (!out.rvalid[pt]) {
+#pragma unroll
+                    for (int k = 0; k < D; ++k) out.nd[(size_t)pt * D + k] = 0.0f;
+                    active = false;
+                    continue;
+                }
+                rprim = out.rprim[pt];
+                rt0 = out.rtuv[2 * (size_t)pt];
+                rt1 = out.rtuv[2 * (size_t)pt + 1];
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    st.p[k] = out.rpt[(size_t)pt * D + k];
+                    rn[k] = out.rnrm[(size_t)pt * D + k];
+                }
+                phase = PH_ND_START;
+            } else {
+                pt = (uint32_t)(idx / c.nwalks);
+                wk = c.walk_offset + (uint32_t)(idx - (long long)pt * c.nwalks);
+                W = (double)__ldg(&dLdu[pt]) / c.nwalks;
+                if (W == 0.0) {
+                    active = false;
+                    continue;
+                }
+                w.start(P + (size_t)pt * D, D);
+                phase = PH_PRIMAL;
+            }
+        }
+        if (!active) continue;
+        if (phase == PH_ND_START) {
+            // no query needed to start: set up the bisection
+            st.uref = dirichlet<D>(S, rprim, rt0, rt1, nullptr, nullptr);
+            ba = a.ball_eps;
+            bb = S.half_min_extent;
+            bk = 0;
+            const float m = (ba + bb) * 0.5f;
+#pragma unroll
+            for (int k = 0; k < D; ++k) qpos[k] = fmaf(rn[k], m, st.p[k]);
+            phase = PH_BALL;
+        }
+        const float *x = (phase == PH_PRIMAL || phase == PH_ANTI_WALK) ? w.p : qpos;
+        const Hit hit = query<D, BVH>(S, x, top, n_top);
+        bool finish_anti = false;
+        float uq = 0.0f;
+        if (phase == PH_PRIMAL) {
+            const int r = walker_advance<D>(w, S, hit, c, c.eps, c.project != 0, c.prevent_fd != 0, pt, wk,
+                                            ROLE_PRIMAL, want_src, cdf);
+            if (r == W_CONTINUE) continue;
+            if (r != W_VALID) {
+                active = false;
+                continue;
+            }
+            const Rec rec = closest_record<D>(S, w.p, hit.prim);
+            rprim = hit.prim;
+            rt0 = rec.t0;
+            rt1 = rec.t1;
+            int vid[3];
+            float wts[3];
+            st.uref = dirichlet<D>(S, rprim, rt0, rt1, vid, wts);
+            if (a.want_dg) {
+#pragma unroll
+                for (int s = 0; s < D; ++s) atomicAdd(&out.dg[vid[s]], W * (double)wts[s]);
+            }
+            if (want_src) {
+#pragma unroll
+                for (int k = 0; k < 5; ++k) acc_src[k] += W * (double)w.ds[k];
+            }
+            if (!a.want_dV) {
+                active = false;
+                continue;
+            }
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                st.p[k] = rec.p[k];
+                rn[k] = rec.n[k];
+            }
+            ba = a.ball_eps;
+            bb = S.half_min_extent;
+            bk = 0;
+            const float m = (ba + bb) * 0.5f;
+#pragma unroll
+            for (int k = 0; k < D; ++k) qpos[k] = fmaf(rn[k], m, st.p[k]);
+            phase = PH_BALL;
+            continue;
+        }
+        if (phase == PH_BALL) {
+            const float d = sqrtf(hit.d2);
+            const float m = (ba + bb) * 0.5f;
+            if (fabsf(d - m) < 1e-5f)
+                ba = m;
+            else
+                bb = m;
+            ++bk;
+            if (bk < 10) {
+                const float m2 = (ba + bb) * 0.5f;
+#pragma unroll
+                for (int k = 0; k < D; ++k) qpos[k] = fmaf(rn[k], m2, st.p[k]);
+                continue;
+            }
+            st.R = ba;
+#pragma unroll
+            for (int k = 0; k < D; ++k) st.n[k] = -rn[k];
+            if (D == 2) st.n[2] = 0.0f;
+            nd_setup<D>(st, S, c, a, pt, wk);
+            nd_point<D>(st, qpos);
+            phase = PH_ANTI_START;
+            continue;
+        }
+        const uint32_t role = st.which == 0 ? ROLE_ANTI_A : ROLE_ANTI_B;
+        if (phase == PH_ANTI_START) {
+            const float d = sqrtf(hit.d2);
+            if (d < a.epsilon2) {
+                const Rec r2 = closest_record<D>(S, qpos, hit.prim);
+                uq = dirichlet<D>(S, hit.prim, r2.t0, r2.t1, nullptr, nullptr);
+                finish_anti = true;
+            } else {
+                w.start(qpos, D);
+                const int r = walker_advance<D>(w, S, hit, c, a.epsilon2, false, false, pt, wk, role, false, cdf);
+                if (r == W_CONTINUE) {
+                    phase = PH_ANTI_WALK;
+                    continue;
+                }
+                if (r == W_VALID) {
+                    const Rec r2 = closest_record<D>(S, w.p, hit.prim);
+                    uq = dirichlet<D>(S, hit.prim, r2.t0, r2.t1, nullptr, nullptr);
+                    if (with_src) uq += w.contrib;
+                }
+                finish_anti = true;
+            }
+        } else {  // PH_ANTI_WALK
+            const int r = walker_advance<D>(w, S, hit, c, a.epsilon2, false, false, pt, wk, role, false, cdf);
+            if (r == W_CONTINUE) continue;
+            if (r == W_VALID) {
+                const Rec r2 = closest_record<D>(S, w.p, hit.prim);
+                uq = dirichlet<D>(S, hit.prim, r2.t0, r2.t1, nullptr, nullptr);
+                if (with_src) uq += w.contrib;
+            }
+            finish_anti = true;
+        }
+        if (finish_anti) {
+            nd_accumulate<D>(st, a, uq);
+            st.which += 1;
+            if (st.which == 1) {
+                nd_point<D>(st, qpos);
+                phase = PH_ANTI_START;
+                continue;
+            }
+            float gn[3];
+            nd_finish<D>(st, S, c, a, pt, wk, with_src, gn);
+            if (ND_ONLY) {
+#pragma unroll
+                for (int k = 0; k < D; ++k) out.nd[(size_t)pt * D + k] = gn[k];
+            } else {
+                float gt[3];
+                tangent_derivative<D>(S, rprim, gt);
+                int vid[3];
+                float wts[3];
+                dirichlet<D>(S, rprim, rt0, rt1, vid, wts);
+#pragma unroll
+                for (int s = 0; s < D; ++s)
+#pragma unroll
+                    for (int k = 0; k < D; ++k)
+                        atomicAdd(&out.dV[(size_t)vid[s] * D + k], W * (double)(-(wts[s] * (gn[k] + gt[k]))));
+            }
+            active = false;
+            phase = PH_IDLE;
+        }
+    }
+    if (want_src) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            double v = acc_src[k];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&out.dsrc[k], v);
+        }
+    }
+}
+
+__global__ void k_add_f64_to_f32(const double *src, float *dst, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] += (float)src[i];
+}
+
+// ------------------------------------------------------------------ host
+static wos_launch_config g_cfg[2] = {{256, 0, 64, 1024}, {256, 0, 32, 768}};
+
+int set_launch_config(int dim, const wos_launch_config *cfg) {
+    if (dim != 2 && dim != 3) return fail(WOS_ERR_INVALID_ARGUMENT, "dim must be 2 or 3");
+    wos_launch_config &c = g_cfg[dim - 2];
+    if (cfg->block_threads) {
+        if (cfg->block_threads % 32 || cfg->block_threads < 32 || cfg->block_threads > 512)
+            return fail(WOS_ERR_INVALID_ARGUMENT, "block_threads must be a multiple of 32 in [32, 512]");
+        c.block_threads = cfg->block_threads;
+    }
+    if (cfg->blocks_per_sm >= 0) c.blocks_per_sm = cfg->blocks_per_sm;
+    if (cfg->chunk) {
+        if (cfg->chunk < 1) return fail(WOS_ERR_INVALID_ARGUMENT, "chunk must be >= 1");
+        c.chunk = cfg->chunk;
+    }
+    if (cfg->smem_nodes >= 0) c.smem_nodes = cfg->smem_nodes;
+    return 0;
+}
+
+int get_launch_config(int dim, wos_launch_config *out) {
+    if (dim != 2 && dim != 3) return fail(WOS_ERR_INVALID_ARGUMENT, "dim must be 2 or 3");
+    *out = g_cfg[dim - 2];
+    return 0;
+}
+
+WalkCfg make_cfg(const wos_params &p) {
+    WalkCfg c;
+    c.nwalks = p.nwalks;
+    c.nsteps = p.nsteps;
+    c.eps = p.epsilon;
+    c.double_sided = p.double_sided;
+    c.prevent_fd = p.prevent_fd_artifacts;
+    c.use_IS = p.use_IS_for_greens;
+    c.include_source = p.include_source;
+    c.project = p.project_unterminated;
+    c.walk_offset = p.walk_offset;
+    c.rng = make_rng(p.seed);
+    return c;
+}
+
+struct Shape {
+    int grid, block, n_top, stage_cdf;
+    size_t smem;
+};
+
+template <typename Kern>
+static int shape_for(Kern kern, const SceneImpl &S, int D, bool bvh, bool want_cdf, Shape &sh) {
+    const wos_launch_config &cfg = g_cfg[D - 2];
+    const int K = D == 2 ? 3 : 4;
+    sh.block = cfg.block_threads;
+    sh.n_top = bvh ? std::min(cfg.smem_nodes, S.nNodes) : 0;
+    sh.stage_cdf = want_cdf ? 1 : 0;
+    sh.smem = (size_t)sh.n_top * K * sizeof(float4) + (want_cdf ? (size_t)S.n_cdf * sizeof(float) : 0);
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)");
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, sh.block, sh.smem);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (occ < 1) return fail(WOS_ERR_UNSUPPORTED, "walk kernel does not fit on an SM with this launch config");
+    const int per_sm = cfg.blocks_per_sm > 0 ? std::min(cfg.blocks_per_sm, occ) : occ;
+    sh.grid = sms * per_sm;
+    return 0;
+}
+
+template <int D, bool BVH>
+static int launch_walk_t(const SceneImpl &S, const float *P, long long total, const wos_params &p, bool records,
+                         const WalkOut &out, unsigned long long *counter, cudaStream_t st) {
+    const SceneView v = S.view();
+    const WalkCfg c = make_cfg(p);
+    const bool want_cdf = D == 2 && S.src_type != 0 && p.use_IS_for_greens;
+    Shape sh;
+    int rc;
+    if (records)
+        rc = shape_for(k_walk<D, BVH, true>, S, D, BVH, want_cdf, sh);
+    else
+        rc = shape_for(k_walk<D, BVH, false>, S, D, BVH, want_cdf, sh);
+    if (rc) return rc;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
+    const int chunk = g_cfg[D - 2].chunk;
+    if (records)
+        k_walk<D, BVH, true><<<sh.grid, sh.block, sh.smem, st>>>(v, c, P, total, counter, chunk, sh.n_top,
+                                                                  sh.stage_cdf, out);
+    else
+        k_walk<D, BVH, false><<<sh.grid, sh.block, sh.smem, st>>>(v, c, P, total, counter, chunk, sh.n_top,
+                                                                   sh.stage_cdf, out);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_walk launch");
+    return 0;
+}
+
+int launch_walk(const SceneImpl &S, const float *P, long long total, const wos_params &p, bool records,
+                const WalkOut &out, unsigned long long *counter, cudaStream_t st) {
+    if (total == 0) return 0;
+    const bool bvh = p.use_bvh != 0;
+    if (S.dim == 2)
+        return bvh ? launch_walk_t<2, true>(S, P, total, p, records, out, counter, st)
+                   : launch_walk_t<2, false>(S, P, total, p, records, out, counter, st);
+    return bvh ? launch_walk_t<3, true>(S, P, total, p, records, out, counter, st)
+               : launch_walk_t<3, false>(S, P, total, p, records, out, counter, st);
+}
+
+int launch_walk_plain(const SceneImpl &S, const float *P, long long total, const wos_params &p, float *values,
+                      cudaStream_t st) {
+    if (total == 0) return 0;
+    const SceneView v = S.view();
+    const WalkCfg c = make_cfg(p);
+    const int B = 256;
+    const long long G = (total + B - 1) / B;
+    const bool bvh = p.use_bvh != 0;
+    if (S.dim == 2) {
+        if (bvh)
+            k_walk_plain<2, true><<<(unsigned)G, B, 0, st>>>(v, c, P, total, values);
+        else
+            k_walk_plain<2, false><<<(unsigned)G, B, 0, st>>>(v, c, P, total, values);
+    } else {
+        if (bvh)
+            k_walk_plain<3, true><<<(unsigned)G, B, 0, st>>>(v, c, P, total, values);
+        else
+            k_walk_plain<3, false><<<(unsigned)G, B, 0, st>>>(v, c, P, total, values);
+    }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_walk_plain launch");
+    return 0;
+}
+
+int launch_reduce(const float *vals, int n, int nw, double *mean, double *var, cudaStream_t st) {
+    if (n == 0) return 0;
+    const int B = 256;
+    const long long G = ((long long)n * 32 + B - 1) / B;
+    k_reduce<<<(unsigned)G, B, 0, st>>>(vals, n, nw, mean, var);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_reduce launch");
+    return 0;
+}
+
+int launch_closest(const SceneImpl &S, const float *P, int n, bool bvh, const QueryOut &o, cudaStream_t st) {
+    if (n == 0) return 0;
+    const SceneView v = S.view();
+    const int B = 128, G = (n + B - 1) / B;
+    if (S.dim == 2) {
+        if (bvh)
+            k_closest<2, true><<<G, B, 0, st>>>(v, P, n, o);
+        else
+            k_closest<2, false><<<G, B, 0, st>>>(v, P, n, o);
+    } else {
+        if (bvh)
+            k_closest<3, true><<<G, B, 0, st>>>(v, P, n, o);
+        else
+            k_closest<3, false><<<G, B, 0, st>>>(v, P, n, o);
+    }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_closest launch");
+    return 0;
+}
+
+int launch_ball(const SceneImpl &S, const uint8_t *valid, const float *pt, const float *nrm, int n, float eps,
+                bool bvh, float *R, cudaStream_t st) {
+    if (n == 0) return 0;
+    const SceneView v = S.view();
+    const int B = 128, G = (n + B - 1) / B;
+    if (S.dim == 2) {
+        if (bvh)
+            k_ball<2, true><<<G, B, 0, st>>>(v, valid, pt, nrm, n, eps, R);
+        else
+            k_ball<2, false><<<G, B, 0, st>>>(v, valid, pt, nrm, n, eps, R);
+    } else {
+        if (bvh)
+            k_ball<3, true><<<G, B, 0, st>>>(v, valid, pt, nrm, n, eps, R);
+        else
+            k_ball<3, false><<<G, B, 0, st>>>(v, valid, pt, nrm, n, eps, R);
+    }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_ball launch");
+    return 0;
+}
+
+template <int D, bool BVH, bool ND>
+static int launch_adjoint_t(const SceneImpl &S, const float *P, long long total, const wos_params &p,
+                            const AdjCfg &a, const float *dLdu, const AdjOut &out, unsigned long long *counter,
+                            cudaStream_t st) {
+    const SceneView v = S.view();
+    const WalkCfg c = make_cfg(p);
+    const bool want_cdf = D == 2 && S.src_type != 0 && p.use_IS_for_greens;
+    Shape sh;
+    int rc = shape_for(k_adjoint<D, BVH, ND>, S, D, BVH, want_cdf, sh);
+    if (rc) return rc;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
+    const int chunk = std::max(1, g_cfg[D - 2].chunk / 2);
+    k_adjoint<D, BVH, ND><<<sh.grid, sh.block, sh.smem, st>>>(v, c, a, P, total, dLdu, counter, chunk, sh.n_top,
+                                                              sh.stage_cdf, out);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_adjoint launch");
+    return 0;
+}
+
+int launch_adjoint(const SceneImpl &S, const float *P, long long total, const wos_params &p, const AdjCfg &a,
+                   const float *dLdu, bool nd_only, const AdjOut &out, unsigned long long *counter, cudaStream_t st) {
+    if (total == 0) return 0;
+    const bool bvh = p.use_bvh != 0;
+#define WOS_ADJ(D_, B_)                                                                               \
+    return nd_only ? launch_adjoint_t<D_, B_, true>(S, P, total, p, a, dLdu, out, counter, st)       \
+                   : launch_adjoint_t<D_, B_, false>(S, P, total, p, a, dLdu, out, counter, st)
+    if (S.dim == 2) {
+        if (bvh) WOS_ADJ(2, true);
+        WOS_ADJ(2, false);
+    }
+    if (bvh) WOS_ADJ(3, true);
+    WOS_ADJ(3, false);
+#undef WOS_ADJ
+}
+
+int launch_add_f64(const double *src, float *dst, long long n, cudaStream_t st) {
+    if (n == 0 || dst == nullptr) return 0;
+    const int B = 256;
+    const int G = (int)std::min<long long>((n + B - 1) / B, 4096);
+    k_add_f64_to_f32<<<G, B, 0, st>>>(src, dst, n);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_add_f64_to_f32 launch");
+    return 0;
+}
+
+}  // namespace wosd

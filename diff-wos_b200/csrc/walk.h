@@ -1,0 +1,70 @@
+// Launch-side interface of the walk kernels (walk.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "scene_impl.h"
+#include "wos_device.cuh"
+
+namespace wosd {
+
+// Device copy of wos_params.
+struct WalkCfg {
+    int nwalks, nsteps;
+    float eps;
+    int double_sided, prevent_fd, use_IS, include_source, project;
+    uint32_t walk_offset;
+    Rng rng;
+};
+
+// Device copy of wos_adjoint_params.
+struct AdjCfg {
+    float epsilon2, clamping;
+    int control_variates, source_in_nd;
+    float ball_eps;
+    int want_dV, want_dg, want_dsrc;
+};
+
+struct WalkOut {
+    float *values;
+    int *steps;
+    uint8_t *valid;
+    float *pt, *nrm, *tuv;
+    int *prim;
+    float *contrib;
+};
+
+struct QueryOut {
+    int *prim;
+    float *dist, *tuv, *pt, *nrm, *sdf;
+    uint8_t *inside;
+};
+
+struct AdjOut {
+    double *dV, *dg, *dsrc;
+    // normal-derivative-only mode: input records and the output estimates
+    const uint8_t *rvalid;
+    const float *rpt, *rnrm, *rtuv;
+    const int *rprim;
+    float *nd;
+};
+
+WalkCfg make_cfg(const wos_params &p);
+int read_status(int reset, int *out);
+int set_launch_config(int dim, const wos_launch_config *cfg);
+int get_launch_config(int dim, wos_launch_config *out);
+
+int launch_walk(const SceneImpl &S, const float *P, long long total, const wos_params &p, bool records,
+                const WalkOut &out, unsigned long long *counter, cudaStream_t st);
+int launch_walk_plain(const SceneImpl &S, const float *P, long long total, const wos_params &p, float *values,
+                      cudaStream_t st);
+int launch_reduce(const float *vals, int n, int nw, double *mean, double *var, cudaStream_t st);
+int launch_closest(const SceneImpl &S, const float *P, int n, bool bvh, const QueryOut &o, cudaStream_t st);
+int launch_ball(const SceneImpl &S, const uint8_t *valid, const float *pt, const float *nrm, int n, float eps,
+                bool bvh, float *R, cudaStream_t st);
+int launch_adjoint(const SceneImpl &S, const float *P, long long total, const wos_params &p, const AdjCfg &a,
+                   const float *dLdu, bool nd_only, const AdjOut &out, unsigned long long *counter, cudaStream_t st);
+int launch_add_f64(const double *src, float *dst, long long n, cudaStream_t st);
+
+}  // namespace wosd

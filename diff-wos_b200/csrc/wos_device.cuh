@@ -1,0 +1,587 @@
+// Device-side scene view, geometry, nearest-primitive queries and samplers
+// for the walk-on-spheres kernels (sm_100a).
+//
+// Arithmetic is written with explicit fmaf() and compiled with -fmad=false,
+// so each function returns the same bits as the CPU oracle's restatement of
+// the same reference function (cited per function).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "wos_math.h"
+
+namespace wosd {
+
+// ------------------------------------------------------------------ status
+// Bits of the device status word (OR-ed by kernels, read by the host).
+enum StatusBits : int {
+    ST_STACK_OVERFLOW = 1,   // BVH traversal stack ran out (result may be wrong)
+    ST_BAD_PRIM       = 2,   // a query returned no primitive
+    ST_NONFINITE      = 4,   // a walk produced a non-finite value
+    ST_QUEUE_LIMIT    = 8,   // a persistent loop hit its iteration limit
+};
+
+// ------------------------------------------------------------------ layout
+// Scene data in HBM.  Primitive data is precomputed once per scene:
+//   2D segment f:   seg[f]  = (a.x, a.y, (b-a).x, (b-a).y), seginv[f] = 1/|b-a|^2
+//   3D triangle f:  tri[3f] = (a.xyz, |ab|^2), tri[3f+1] = (ab.xyz, ab.ac),
+//                   tri[3f+2] = (ac.xyz, |ac|^2)
+// The LBVH (Karras, leaf size 1) is stored breadth-first; node k holds the
+// boxes of both children and the two child references:
+//   2D: node[3k] = (L.lo, L.hi), node[3k+1] = (R.lo, R.hi), node[3k+2].xy = refs
+//   3D: node[4k..4k+2] = (L.lo.xyz, L.hi.xyz, R.lo.xyz, R.hi.xyz) packed,
+//       node[4k+3].xy = refs
+// A reference r >= 0 is an internal node, r < 0 is leaf ~r in Morton order;
+// leaf data is copied into Morton order (lseg/lseginv/ltri) with the original
+// primitive index in lorig.
+struct SceneView {
+    int dim, nV, nF;
+    const float *V;    // nV x dim
+    const int *F;      // nF x dim
+    const float *N;    // vertex normals, nV x dim
+    const float *g;    // Dirichlet values, nV
+    const float4 *seg;
+    const float *seginv;
+    const float4 *tri;
+    int nNodes;
+    const float4 *node;
+    const float4 *lseg;
+    const float *lseginv;
+    const float4 *ltri;
+    const int *lorig;
+    float lo[3], hi[3];
+    float half_min_extent;  // min_k (hi_k - lo_k) / 2
+    int src_type;
+    float src[5];
+    const float *cdf;  // G CDF table (n_cdf entries)
+    int n_cdf;
+};
+
+template <int D>
+struct NodeWords;
+template <>
+struct NodeWords<2> {
+    static constexpr int K = 3;
+};
+template <>
+struct NodeWords<3> {
+    static constexpr int K = 4;
+};
+
+// ------------------------------------------------------------------ Philox
+// Philox-4x32-10 (Salmon et al., SC 2011); counter = (point, walk, step, role).
+struct Rng {
+    uint32_t k0, k1;
+};
+
+__host__ __device__ inline Rng make_rng(uint64_t seed) {
+    return Rng{(uint32_t)seed, (uint32_t)(seed >> 32) ^ 0x5bd1e995u};
+}
+
+__device__ __forceinline__ uint4 philox(Rng key, uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3) {
+    uint32_t k0 = key.k0, k1 = key.k1;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+        const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return make_uint4(c0, c1, c2, c3);
+}
+
+enum { ROLE_PRIMAL = 0, ROLE_ANTI_A = 1, ROLE_ANTI_B = 2, ROLE_EXTRA = 3 };
+
+// ------------------------------------------------------------------ vectors
+__device__ __forceinline__ float dot2(float ax, float ay, float bx, float by) { return fmaf(ax, bx, ay * by); }
+__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+    return fmaf(ax, bx, fmaf(ay, by, az * bz));
+}
+__device__ __forceinline__ void cross3(float ax, float ay, float az, float bx, float by, float bz, float &ox,
+                                       float &oy, float &oz) {
+    ox = ay * bz - az * by;
+    oy = az * bx - ax * bz;
+    oz = ax * by - ay * bx;
+}
+
+// ------------------------------------------------------------------ geometry
+// Squared distance from p to a segment (include/util.cuh:108-114), with the
+// clamped parameter h.
+__device__ __forceinline__ float seg_d2(float4 s, float inv, float px, float py, float &h) {
+    const float pax = px - s.x, pay = py - s.y;
+    float t = dot2(pax, pay, s.z, s.w) * inv;
+    t = fminf(fmaxf(t, 0.0f), 1.0f);
+    const float vx = fmaf(-s.z, t, pax), vy = fmaf(-s.w, t, pay);
+    h = t;
+    return dot2(vx, vy, vx, vy);
+}
+
+// Closest point on a triangle (include/util.cuh:22-106, Ericson's Voronoi
+// regions), in terms of a, ab, ac and the precomputed dot products.
+// Returns the squared distance; (v, w) weight b and c; (dx, dy, dz) = x - pt.
+__device__ __forceinline__ float tri_closest(float4 t0, float4 t1, float4 t2, float x, float y, float z, float &v,
+                                             float &w, float &dx, float &dy, float &dz) {
+    const float axx = x - t0.x, axy = y - t0.y, axz = z - t0.z;
+    const float ab2 = t0.w, abac = t1.w, ac2 = t2.w;
+    const float d1 = dot3(t1.x, t1.y, t1.z, axx, axy, axz);
+    const float d2 = dot3(t2.x, t2.y, t2.z, axx, axy, axz);
+    if (d1 <= 0.0f && d2 <= 0.0f) {
+        v = 0.0f;
+        w = 0.0f;
+    } else {
+        const float d3 = d1 - ab2, d4 = d2 - abac;
+        if (d3 >= 0.0f && d4 <= d3) {
+            v = 1.0f;
+            w = 0.0f;
+        } else {
+            const float d5 = d1 - abac, d6 = d2 - ac2;
+            if (d6 >= 0.0f && d5 <= d6) {
+                v = 0.0f;
+                w = 1.0f;
+            } else {
+                const float vc = d1 * d4 - d3 * d2;
+                if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+                    v = d1 / (d1 - d3);
+                    w = 0.0f;
+                } else {
+                    const float vb = d5 * d2 - d1 * d6;
+                    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+                        v = 0.0f;
+                        w = d2 / (d2 - d6);
+                    } else {
+                        const float va = d3 * d6 - d5 * d4;
+                        const float e43 = d4 - d3, e56 = d5 - d6;
+                        if (va <= 0.0f && e43 >= 0.0f && e56 >= 0.0f) {
+                            w = e43 / (e43 + e56);
+                            v = 1.0f - w;
+                        } else {
+                            const float sum = va + vb + vc;
+                            if (sum > 0.0f) {
+                                const float denom = 1.0f / sum;
+                                v = vb * denom;
+                                w = vc * denom;
+                            } else {
+                                v = 0.0f;
+                                w = 0.0f;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    dx = fmaf(-t2.x, w, fmaf(-t1.x, v, axx));
+    dy = fmaf(-t2.y, w, fmaf(-t1.y, v, axy));
+    dz = fmaf(-t2.z, w, fmaf(-t1.z, v, axz));
+    return dot3(dx, dy, dz, dx, dy, dz);
+}
+
+__device__ __forceinline__ float tri_d2(float4 t0, float4 t1, float4 t2, float x, float y, float z) {
+    float v, w, dx, dy, dz;
+    return tri_closest(t0, t1, t2, x, y, z, v, w, dx, dy, dz);
+}
+
+// ------------------------------------------------------------------ queries
+struct Hit {
+    int prim;
+    float d2;
+};
+
+// Pruning slack (same rule as the oracle): a box is skipped only when its
+// squared distance exceeds (1 + 2^-10) best + 1025 (s 2^-20)^2, where s
+// bounds the coordinates' magnitude around the scene.
+template <int D>
+__device__ __forceinline__ float prune_tol2(const SceneView &S, const float *p) {
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < D; ++k) s = fmaxf(s, S.hi[k] - S.lo[k]);
+#pragma unroll
+    for (int k = 0; k < D; ++k) s += fabsf(p[k] - (S.lo[k] + S.hi[k]) * 0.5f);
+    const float e = s * 9.5367431640625e-07f;
+    return 1025.0f * (e * e);
+}
+__device__ __forceinline__ float prune_bound(float best, float tol2) { return fmaf(best, 1.0009765625f, tol2); }
+
+// Brute-force nearest over the original primitive order, ties to the lowest
+// index (include/scene.cuh:102-128).
+template <int D>
+__device__ __forceinline__ Hit nearest_brute(const SceneView &S, const float *p) {
+    Hit h{-1, INFINITY};
+    if (D == 2) {
+        for (int f = 0; f < S.nF; ++f) {
+            float t;
+            const float d2 = seg_d2(__ldg(&S.seg[f]), __ldg(&S.seginv[f]), p[0], p[1], t);
+            if (d2 < h.d2) {
+                h.d2 = d2;
+                h.prim = f;
+            }
+        }
+    } else {
+        for (int f = 0; f < S.nF; ++f) {
+            const float d2 = tri_d2(__ldg(&S.tri[3 * f]), __ldg(&S.tri[3 * f + 1]), __ldg(&S.tri[3 * f + 2]), p[0],
+                                    p[1], p[2]);
+            if (d2 < h.d2) {
+                h.d2 = d2;
+                h.prim = f;
+            }
+        }
+    }
+    return h;
+}
+
+template <int D>
+__device__ __forceinline__ float box_d2(const float *lo, const float *hi, const float *p) {
+    float d[3];
+#pragma unroll
+    for (int k = 0; k < D; ++k) d[k] = fmaxf(fmaxf(lo[k] - p[k], p[k] - hi[k]), 0.0f);
+    return D == 2 ? fmaf(d[0], d[0], d[1] * d[1]) : fmaf(d[0], d[0], fmaf(d[1], d[1], d[2] * d[2]));
+}
+
+template <int D>
+__device__ __forceinline__ void load_node(const float4 *base, int k, float (*lo)[3], float (*hi)[3], int &c0,
+                                          int &c1) {
+    if (D == 2) {
+        const float4 a = base[3 * k], b = base[3 * k + 1], c = base[3 * k + 2];
+        lo[0][0] = a.x;
+        lo[0][1] = a.y;
+        hi[0][0] = a.z;
+        hi[0][1] = a.w;
+        lo[1][0] = b.x;
+        lo[1][1] = b.y;
+        hi[1][0] = b.z;
+        hi[1][1] = b.w;
+        c0 = __float_as_int(c.x);
+        c1 = __float_as_int(c.y);
+    } else {
+        const float4 a = base[4 * k], b = base[4 * k + 1], c = base[4 * k + 2], e = base[4 * k + 3];
+        lo[0][0] = a.x;
+        lo[0][1] = a.y;
+        lo[0][2] = a.z;
+        hi[0][0] = a.w;
+        hi[0][1] = b.x;
+        hi[0][2] = b.y;
+        lo[1][0] = b.z;
+        lo[1][1] = b.w;
+        lo[1][2] = c.x;
+        hi[1][0] = c.y;
+        hi[1][1] = c.z;
+        hi[1][2] = c.w;
+        c0 = __float_as_int(e.x);
+        c1 = __float_as_int(e.y);
+    }
+}
+
+#ifndef WOS_STACK
+#define WOS_STACK 64
+#endif
+
+// LBVH nearest: nearest-first descent with a per-thread stack, conservative
+// pruning, ties to the lowest original index.  The first n_top nodes (the
+// shallowest, breadth-first) are read from shared memory.
+template <int D>
+__device__ __forceinline__ Hit nearest_bvh(const SceneView &S, const float *p, const float4 *top, int n_top,
+                                           int *status) {
+    Hit h{-1, INFINITY};
+    if (S.nF == 1) {
+        h.prim = 0;
+        if (D == 2) {
+            float t;
+            h.d2 = seg_d2(__ldg(&S.seg[0]), __ldg(&S.seginv[0]), p[0], p[1], t);
+        } else {
+            h.d2 = tri_d2(__ldg(&S.tri[0]), __ldg(&S.tri[1]), __ldg(&S.tri[2]), p[0], p[1], p[2]);
+        }
+        return h;
+    }
+    const float tol2 = prune_tol2<D>(S, p);
+    int stn[WOS_STACK];
+    float std2[WOS_STACK];
+    int sp = 1;
+    stn[0] = 0;
+    std2[0] = 0.0f;
+    int best_leaf = -1;
+    while (sp > 0) {
+        --sp;
+        const int v = stn[sp];
+        if (std2[sp] > prune_bound(h.d2, tol2)) continue;
+        float lo[2][3], hi[2][3];
+        int ch[2];
+        if (v < n_top)
+            load_node<D>(top, v, lo, hi, ch[0], ch[1]);
+        else
+            load_node<D>(S.node, v, lo, hi, ch[0], ch[1]);
+        float bd[2];
+        bd[0] = box_d2<D>(lo[0], hi[0], p);
+        bd[1] = box_d2<D>(lo[1], hi[1], p);
+        const int nr = bd[1] < bd[0] ? 1 : 0;
+        const int cn = nr ? ch[1] : ch[0], cf = nr ? ch[0] : ch[1];
+        const float dn = nr ? bd[1] : bd[0], df = nr ? bd[0] : bd[1];
+#pragma unroll
+        for (int pass = 0; pass < 2; ++pass) {
+            const int c = pass == 0 ? cn : cf;
+            const float bdc = pass == 0 ? dn : df;
+            if (c < 0 && bdc <= prune_bound(h.d2, tol2)) {
+                const int leaf = ~c;
+                float d2;
+                if (D == 2) {
+                    float t;
+                    d2 = seg_d2(__ldg(&S.lseg[leaf]), __ldg(&S.lseginv[leaf]), p[0], p[1], t);
+                } else {
+                    d2 = tri_d2(__ldg(&S.ltri[3 * leaf]), __ldg(&S.ltri[3 * leaf + 1]), __ldg(&S.ltri[3 * leaf + 2]),
+                                p[0], p[1], p[2]);
+                }
+                if (d2 <= h.d2) {
+                    const int orig = __ldg(&S.lorig[leaf]);
+                    if (d2 < h.d2 || orig < h.prim) {
+                        h.d2 = d2;
+                        h.prim = orig;
+                        best_leaf = leaf;
+                    }
+                }
+            }
+        }
+        if (cf >= 0 && df <= prune_bound(h.d2, tol2)) {
+            if (sp < WOS_STACK) {
+                stn[sp] = cf;
+                std2[sp] = df;
+                ++sp;
+            } else {
+                atomicOr(status, ST_STACK_OVERFLOW);
+            }
+        }
+        if (cn >= 0 && dn <= prune_bound(h.d2, tol2)) {
+            if (sp < WOS_STACK) {
+                stn[sp] = cn;
+                std2[sp] = dn;
+                ++sp;
+            } else {
+                atomicOr(status, ST_STACK_OVERFLOW);
+            }
+        }
+    }
+    (void)best_leaf;
+    return h;
+}
+
+// ------------------------------------------------------------------ records
+// Closest-point record at x for primitive prim (include/scene.cuh:180-223).
+struct Rec {
+    float p[3];
+    float n[3];
+    float t0, t1;  // 2D: (h, 0); 3D: (w_b, w_c)
+};
+
+template <int D>
+__device__ __forceinline__ Rec closest_record(const SceneView &S, const float *x, int prim) {
+    Rec r;
+    if (D == 2) {
+        const float4 s = __ldg(&S.seg[prim]);
+        float h;
+        seg_d2(s, __ldg(&S.seginv[prim]), x[0], x[1], h);
+        const float pax = x[0] - s.x, pay = x[1] - s.y;
+        r.p[0] = fmaf(s.z, h, s.x);
+        r.p[1] = fmaf(s.w, h, s.y);
+        float nx = s.w, ny = -s.z;
+        const float len = sqrtf(dot2(nx, ny, nx, ny));
+        nx = nx / len;
+        ny = ny / len;
+        if (!(dot2(nx, ny, pax, pay) > 0.0f)) {
+            nx = -nx;
+            ny = -ny;
+        }
+        r.n[0] = nx;
+        r.n[1] = ny;
+        r.n[2] = 0.0f;
+        r.p[2] = 0.0f;
+        r.t0 = h;
+        r.t1 = 0.0f;
+    } else {
+        const float4 t0 = __ldg(&S.tri[3 * prim]), t1 = __ldg(&S.tri[3 * prim + 1]), t2 = __ldg(&S.tri[3 * prim + 2]);
+        float v, w, dx, dy, dz;
+        tri_closest(t0, t1, t2, x[0], x[1], x[2], v, w, dx, dy, dz);
+        r.p[0] = fmaf(t2.x, w, fmaf(t1.x, v, t0.x));
+        r.p[1] = fmaf(t2.y, w, fmaf(t1.y, v, t0.y));
+        r.p[2] = fmaf(t2.z, w, fmaf(t1.z, v, t0.z));
+        float nx, ny, nz;
+        cross3(t1.x, t1.y, t1.z, t2.x, t2.y, t2.z, nx, ny, nz);
+        const float len = sqrtf(dot3(nx, ny, nz, nx, ny, nz));
+        nx = nx / len;
+        ny = ny / len;
+        nz = nz / len;
+        const float axx = x[0] - t0.x, axy = x[1] - t0.y, axz = x[2] - t0.z;
+        const float sg = dot3(nx, ny, nz, axx, axy, axz) > 0.0f ? 1.0f : -1.0f;
+        r.n[0] = sg * nx;
+        r.n[1] = sg * ny;
+        r.n[2] = sg * nz;
+        r.t0 = v;
+        r.t1 = w;
+    }
+    return r;
+}
+
+// Signed distance and inside test (same composition as the oracle:
+// include/scene.cuh:148-178 with wos/scene.py:325-339 and
+// wos/scene3d.py:201-214).
+template <int D>
+__device__ __forceinline__ bool inside_test(const SceneView &S, const float *p, const Hit &hit, float *sd) {
+    if (hit.prim < 0) {
+        if (sd) *sd = INFINITY;
+        return false;
+    }
+    const float d = sqrtf(hit.d2);
+    if (D == 2) {
+        const float4 s = __ldg(&S.seg[hit.prim]);
+        float h;
+        seg_d2(s, __ldg(&S.seginv[hit.prim]), p[0], p[1], h);
+        const float pax = p[0] - s.x, pay = p[1] - s.y;
+        const float vx = fmaf(-s.z, h, pax), vy = fmaf(-s.w, h, pay);
+        const int ia = __ldg(&S.F[2 * hit.prim]), ib = __ldg(&S.F[2 * hit.prim + 1]);
+        const float nax = __ldg(&S.N[2 * ia]), nay = __ldg(&S.N[2 * ia + 1]);
+        const float nbx = __ldg(&S.N[2 * ib]), nby = __ldg(&S.N[2 * ib + 1]);
+        const float nx = fmaf(nbx - nax, h, nax), ny = fmaf(nby - nay, h, nay);
+        const float s2 = dot2(nx, ny, vx, vy);
+        if (sd) *sd = s2 > 0.0f ? d : -d;
+        return (s2 < 0.0f) && (hit.d2 > 0.0f);
+    } else {
+        const float4 t0 = __ldg(&S.tri[3 * hit.prim]), t1 = __ldg(&S.tri[3 * hit.prim + 1]),
+                     t2 = __ldg(&S.tri[3 * hit.prim + 2]);
+        float v, w, dx, dy, dz;
+        tri_closest(t0, t1, t2, p[0], p[1], p[2], v, w, dx, dy, dz);
+        float fx, fy, fz;
+        cross3(t1.x, t1.y, t1.z, t2.x, t2.y, t2.z, fx, fy, fz);
+        const float sf = dot3(fx, fy, fz, dx, dy, dz);
+        const int ia = __ldg(&S.F[3 * hit.prim]), ib = __ldg(&S.F[3 * hit.prim + 1]),
+                  ic = __ldg(&S.F[3 * hit.prim + 2]);
+        const float w0 = (1.0f - v) - w;
+        float nv[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            nv[k] = fmaf(__ldg(&S.N[3 * ia + k]), w0, fmaf(__ldg(&S.N[3 * ib + k]), v, __ldg(&S.N[3 * ic + k]) * w));
+        const float sv = dot3(nv[0], nv[1], nv[2], dx, dy, dz);
+        if (sd) *sd = sf > 0.0f ? d : -d;
+        return (hit.d2 > 0.0f) && (sv < 0.0f) && (sf <= 0.0f);
+    }
+}
+
+// Dirichlet value (include/scene.cuh:251-264) and the vertex weights.
+template <int D>
+__device__ __forceinline__ float dirichlet(const SceneView &S, int prim, float t0, float t1, int *vid, float *wts) {
+    if (D == 2) {
+        const int ia = __ldg(&S.F[2 * prim]), ib = __ldg(&S.F[2 * prim + 1]);
+        const float va = __ldg(&S.g[ia]), vb = __ldg(&S.g[ib]);
+        if (vid) {
+            vid[0] = ia;
+            vid[1] = ib;
+            wts[0] = 1.0f - t0;
+            wts[1] = t0;
+        }
+        return fmaf(t0, vb - va, va);
+    } else {
+        const int ia = __ldg(&S.F[3 * prim]), ib = __ldg(&S.F[3 * prim + 1]), ic = __ldg(&S.F[3 * prim + 2]);
+        const float va = __ldg(&S.g[ia]), vb = __ldg(&S.g[ib]), vc = __ldg(&S.g[ic]);
+        const float w0 = (1.0f - t0) - t1;
+        if (vid) {
+            vid[0] = ia;
+            vid[1] = ib;
+            vid[2] = ic;
+            wts[0] = w0;
+            wts[1] = t0;
+            wts[2] = t1;
+        }
+        return fmaf(va, w0, fmaf(vb, t0, vc * t1));
+    }
+}
+
+// Source function and its parameter derivatives (include/scene.cuh:278-301).
+__device__ __forceinline__ float source(const SceneView &S, float x, float y, float *df) {
+    const float *q = S.src;
+    if (S.src_type == 1) {
+        const float tx = x - q[0], ty = y - q[1];
+        const float sx2 = q[2] * q[2], sy2 = q[3] * q[3];
+        const float dx = tx * tx / (2.0f * sx2);
+        const float dy = ty * ty / (2.0f * sy2);
+        const float E = wosm::exp_(-dx - dy);
+        const float f = q[4] * E;
+        if (df) {
+            df[0] = f * (tx / sx2);
+            df[1] = f * (ty / sy2);
+            df[2] = f * (tx * tx / (sx2 * q[2]));
+            df[3] = f * (ty * ty / (sy2 * q[3]));
+            df[4] = E;
+        }
+        return f;
+    }
+    if (S.src_type == 2) {
+        const float phi = fmaf(q[0], x, fmaf(q[1], y, q[2]));
+        const float s = wosm::sin_(phi);
+        if (df) {
+            const float c = wosm::cos_(phi);
+            df[0] = q[3] * c * x;
+            df[1] = q[3] * c * y;
+            df[2] = q[3] * c;
+            df[3] = s;
+            df[4] = 1.0f;
+        }
+        return fmaf(q[3], s, q[4]);
+    }
+    if (df) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) df[k] = 0.0f;
+    }
+    return 0.0f;
+}
+
+// Radius sample from the G CDF (include/wos.cuh:49-75); cdf may point to
+// shared memory.
+__device__ __forceinline__ float sample_G_radius(const float *cdf, int n, float u, float R, float &pdf) {
+    int l = 0, r = n - 1;
+    while (l < r) {
+        const int mid = (l + r) >> 1;
+        if (u < cdf[mid])
+            r = mid;
+        else
+            l = mid + 1;
+    }
+    const float pmf = l == 0 ? cdf[0] : cdf[l] - cdf[l - 1];
+    const float prev = l == 0 ? 0.0f : cdf[l - 1];
+    u = (u - prev) / pmf;
+    pdf = pmf * (float)n / R;
+    return R * ((float)l + u) / (float)n;
+}
+
+// Interior source term of one step (include/wos.cuh:115-139 with the
+// importance-sampled branch of :121-130): returns the factor K with
+// contrib += f(y) * K, and y.
+__device__ __forceinline__ float source_step(const SceneView &S, const float *cdf, bool use_IS, float px, float py,
+                                             float d, uint32_t ra, uint32_t rb, float &yx, float &yy) {
+    float dx, dy, pdf, weight;
+    if (use_IS) {
+        const float rad = sample_G_radius(cdf, S.n_cdf, wosm::u01(ra), d, pdf);
+        float s, c;
+        wosm::sincos_2pi(wosm::u01(rb), &s, &c);
+        pdf = pdf / wosm::kTwoPi;
+        dx = rad * c;
+        dy = rad * s;
+        weight = sqrtf(dot2(dx, dy, dx, dy));
+    } else {
+        float s, c;
+        wosm::sincos_2pi(wosm::u01(ra), &s, &c);
+        const float rr = sqrtf(wosm::u01(rb));
+        dx = rr * c * d;
+        dy = rr * s * d;
+        pdf = 1.0f / (wosm::kPi * d * d);
+        weight = 1.0f;
+    }
+    const float rn = sqrtf(dot2(dx, dy, dx, dy));
+    const float G = wosm::log_(d / fmaxf(rn, 1e-4f)) * wosm::kInv2Pi;
+    yx = px + dx;
+    yy = py + dy;
+    return pdf > 1e-5f ? G * weight / pdf : 0.0f;
+}
+
+}  // namespace wosd

@@ -1,0 +1,15 @@
+"""3D gradient solver (reference: wos/wos_grad_3d.py:378-411)."""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+from .wos_grad import OursCUDA
+
+
+@dataclass
+class Ours3D(OursCUDA):
+    """Boundary-shape estimator on triangle meshes: the 3D normal derivative
+    (wos/wos3d.py:248-286) plus the face tangential derivative
+    (wos/wos3d.py:288-307)."""
+    epsilon2: float = 1e-3
+    clamping: float = 1e-1

@@ -1,0 +1,255 @@
+/*
+ * wos_b200.h -- C ABI of the B200 walk-on-spheres library (libwos_b200.so).
+ *
+ * This is the drop-in boundary for the hot path of diff-wos.  It replaces the
+ * reference's pybind module `wos_ext` (src/python/main.cpp:9-17,
+ * src/python/scene.cu:10-88, src/python/wos.cu:5-25), whose arguments were
+ * Dr.Jit CUDA arrays, with plain pointers and sizes:
+ *
+ *   - every array argument is a pointer to DEVICE memory of the current CUDA
+ *     device (for example a torch CUDA tensor's data_ptr()), C-contiguous;
+ *     points and vertices are n x dim float32, faces are nF x dim int32;
+ *   - every call takes the cudaStream_t it runs on and is asynchronous on it,
+ *     except wos_scene_create / wos_scene_update_vertices, which return
+ *     after the scene is built;
+ *   - every call returns 0 on success or a negative WOS_ERR_* code, and
+ *     wos_last_error_string() describes the last failure of this thread;
+ *   - a scene handle is immutable between wos_scene_update_* calls and may be
+ *     used by concurrent launches on different streams.
+ *
+ * Randomness is counter based: a walk's random numbers are Philox-4x32-10 of
+ * (seed; point index, walk index, step, role), so results do not depend on
+ * launch shape, scheduling or how many walks run per call.
+ */
+#ifndef WOS_B200_H
+#define WOS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define WOS_API __attribute__((visibility("default")))
+#else
+#define WOS_API
+#endif
+
+typedef struct CUstream_st *wos_stream_t; /* == cudaStream_t */
+typedef struct wos_scene_s *wos_scene_t;
+
+enum {
+    WOS_OK = 0,
+    WOS_ERR_INVALID_ARGUMENT = -1,
+    WOS_ERR_CUDA = -2,
+    WOS_ERR_EMPTY_SCENE = -3,
+    WOS_ERR_UNSUPPORTED = -4,
+    WOS_ERR_WORKSPACE = -5,
+};
+
+/* Device status bits OR-ed by kernels (wos_device_status). */
+enum {
+    WOS_STATUS_STACK_OVERFLOW = 1,
+    WOS_STATUS_BAD_PRIM = 2,
+    WOS_STATUS_NONFINITE = 4,
+    WOS_STATUS_QUEUE_LIMIT = 8,
+};
+
+/* Solver settings.  Mirrors wos_ext.WoS / WoS3D(nwalks, nsteps=32,
+ * epsilon=1e-3, double_sided=False, prevent_fd_artifacts=False,
+ * use_IS_for_greens) (src/python/wos.cu:9-12) plus:
+ *   include_source       add the interior source term to each walk's value
+ *                        (WoSWithSourceCUDA.single_walk,
+ *                        wos/wos_with_source.py:257-265); 0 gives the
+ *                        WoSCUDA value (wos/wos.py:171-179);
+ *   project_unterminated 0: a walk that reaches nsteps is invalid and scores 0
+ *                        (include/wos.cuh:144); 1: it is projected to its
+ *                        closest boundary point (the Dr.Jit walk, wos/wos.py:43);
+ *   use_bvh              1: LBVH nearest queries, 0: brute force
+ *                        (include/scene.cuh:150-154);
+ *   walk_offset          first walk index (the sampler's position);
+ *   seed                 64-bit Philox key. */
+typedef struct wos_params {
+    int32_t nwalks;
+    int32_t nsteps;
+    float epsilon;
+    int32_t double_sided;
+    int32_t prevent_fd_artifacts;
+    int32_t use_IS_for_greens;
+    int32_t include_source;
+    int32_t project_unterminated;
+    int32_t use_bvh;
+    uint32_t walk_offset;
+    uint64_t seed;
+} wos_params;
+
+/* Settings of the differential estimator (OursCUDA / Ours3D,
+ * wos/wos_grad.py:113-151, wos/wos_grad_3d.py:378-411):
+ *   epsilon2                    shell width of the walks on the inscribed ball;
+ *   clamping                    angle clamp of the off-centred Poisson kernel;
+ *   control_variates            subtract u at the boundary point (wos/wos.py:227);
+ *   source_in_normal_derivative use the source-aware normal derivative
+ *                               (wos/wos_with_source.py:154-232) when the
+ *                               scene has a source (2D);
+ *   ball_epsilon                lower bound of the inscribed-ball bisection
+ *                               (include/scene.cuh:225, default 1e-3);
+ *   want_dV / want_dg / want_dsrc  which gradients to accumulate. */
+typedef struct wos_adjoint_params {
+    float epsilon2;
+    float clamping;
+    int32_t control_variates;
+    int32_t source_in_normal_derivative;
+    float ball_epsilon;
+    int32_t want_dV;
+    int32_t want_dg;
+    int32_t want_dsrc;
+} wos_adjoint_params;
+
+typedef struct wos_scene_info {
+    int32_t dim, n_vertices, n_faces, n_nodes, bvh_depth, source_type;
+    float aabb_min[3], aabb_max[3];
+    float source_params[5];
+} wos_scene_info;
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+WOS_API int wos_version(void);
+
+/* Message of this thread's last failing call ("" if none). */
+WOS_API const char *wos_last_error_string(void);
+
+/* Device status word of the current device; reset != 0 clears it.  Reading it
+ * synchronises the device. */
+WOS_API int wos_device_status(int reset, int32_t *out);
+
+/* ---------------------------------------------------------------- scenes */
+
+/* Build a scene: copies vertices V (nV x dim), faces F (nF x dim, CCW
+ * polylines / outward-oriented triangles), Dirichlet values g (nV); computes
+ * vertex normals, the AABB and the LBVH.  source_params is a HOST array of 5
+ * floats (NULL for none).  Replaces wos_ext.Scene(vertices, indices, values,
+ * use_bvh[, source_type, source_params]) / Scene3D (src/python/scene.cu:28-83,
+ * include/scene.cuh:330-453).  Returns after the build completes. */
+WOS_API int wos_scene_create(int dim, const float *V, int nV, const int *F, int nF, const float *g, int source_type,
+                     const float *source_params, wos_stream_t stream, wos_scene_t *out);
+
+/* Free a scene (stream-ordered on `stream`). */
+WOS_API int wos_scene_destroy(wos_scene_t scene, wos_stream_t stream);
+
+/* Replace the Dirichlet values (nV floats, device).  The scene's `values`
+ * field (src/python/scene.cu:38). */
+WOS_API int wos_scene_update_values(wos_scene_t scene, const float *g, wos_stream_t stream);
+
+/* Replace vertex positions (nV x dim, device) and rebuild normals, AABB and
+ * LBVH; returns after the rebuild. */
+WOS_API int wos_scene_update_vertices(wos_scene_t scene, const float *V, wos_stream_t stream);
+
+/* Set the analytic source (include/scene.cuh:270-301): type 0 none,
+ * 1 Gaussian (mu_x, mu_y, sigma_x, sigma_y, A), 2 sinusoid
+ * (A, B, C, amplitude, offset) = amplitude * sin(A x + B y + C) + offset.
+ * params is a HOST array of 5 floats.  The walk solves -Lap u = f. */
+WOS_API int wos_scene_set_source(wos_scene_t scene, int source_type, const float *params);
+
+WOS_API int wos_scene_get_info(wos_scene_t scene, wos_scene_info *out);
+
+/* Copy the vertex normals (nV x dim, device) into out (device). */
+WOS_API int wos_scene_get_normals(wos_scene_t scene, float *out, wos_stream_t stream);
+
+/* ---------------------------------------------------------------- queries */
+
+/* Closest boundary point of n points P (n x dim): Scene.closest_point_preliminary
+ * (include/scene.cuh:102-146), closest_point (:180-223) and sdf (:148-178).
+ * Any output may be NULL.  prim: nearest primitive (ties to the lowest index);
+ * dist: unsigned distance; t_or_uv: n x 2 (2D: (t, 0), 3D: (w_b, w_c));
+ * pt, normal: n x dim (normal oriented towards the query point);
+ * sdf: signed distance (negative inside); inside: 1 if the point is inside
+ * (the test that gates a walk). */
+WOS_API int wos_closest_point(wos_scene_t scene, const float *P, int n, int use_bvh, int32_t *prim, float *dist,
+                      float *t_or_uv, float *pt, float *normal, float *sdf, uint8_t *inside, wos_stream_t stream);
+
+/* Scene.largest_inscribed_ball(its, epsilon) (include/scene.cuh:225-249,
+ * :659-704): 10-step bisection of the ball tangent at boundary point pt with
+ * inward normal `normal`; R = 0 where valid == 0. */
+WOS_API int wos_largest_inscribed_ball(wos_scene_t scene, const uint8_t *valid, const float *pt, const float *normal, int n,
+                               float epsilon, int use_bvh, float *R, wos_stream_t stream);
+
+/* ---------------------------------------------------------------- walks */
+
+/* One walk per point with walk index p->walk_offset; the record of
+ * WoS.single_walk(p, scene, sampler) (include/wos.cuh:374-533).  valid: n;
+ * pt, normal: n x dim; t_or_uv: n x 2; prim: n (-1 if invalid); contrib: n
+ * (source term).  Any output except valid may be NULL. */
+WOS_API int wos_walk_records(wos_scene_t scene, const float *P, int n, const wos_params *p, uint8_t *valid, float *pt,
+                     float *normal, float *t_or_uv, int32_t *prim, float *contrib, wos_stream_t stream);
+
+/* Per-walk values: values[i * nwalks + w] = value of walk w of point i
+ * (0 for an invalid walk).  steps (may be NULL): steps per walk. */
+WOS_API int wos_walk_values(wos_scene_t scene, const float *P, int n, const wos_params *p, float *values, int32_t *steps,
+                    wos_stream_t stream);
+
+/* Workspace bytes for wos_solve with n points. */
+WOS_API size_t wos_solve_workspace_size(int n, const wos_params *p);
+
+/* Solver.walk / solve (wos/solver.py:41-65): per-point mean over nwalks
+ * walks and the sample variance of the per-walk values, reduced in FP64
+ * with compensated sums.  var may be NULL.  workspace may be NULL (then it
+ * is allocated stream-ordered) or point to wos_solve_workspace_size bytes of
+ * device memory. */
+WOS_API int wos_solve(wos_scene_t scene, const float *P, int n, const wos_params *p, double *mean, double *var,
+              void *workspace, size_t workspace_bytes, wos_stream_t stream);
+
+/* ---------------------------------------------------------------- gradients */
+
+/* WoS.normal_derivative(its, scene, sampler, clamping, control_variates)
+ * (wos/wos.py:184-232; with source wos/wos_with_source.py:154-232; 3D
+ * wos/wos3d.py:248-286): one estimate per record, returned as grad * n_out
+ * (n x dim).  Records as from wos_walk_records; walk index p->walk_offset. */
+WOS_API int wos_normal_derivative(wos_scene_t scene, const uint8_t *valid, const float *pt, const float *normal,
+                          const float *t_or_uv, const int32_t *prim, int n, const wos_params *p,
+                          const wos_adjoint_params *a, float *out, wos_stream_t stream);
+
+/* Workspace bytes for wos_adjoint on this scene. */
+WOS_API size_t wos_adjoint_workspace_size(wos_scene_t scene);
+
+/* Reverse-mode derivative of the per-point means of wos_solve with respect
+ * to vertex positions (dV, nV x dim), Dirichlet values (dg, nV) and source
+ * parameters (dsrc, 5): out += sum_i dLdu[i] d mean_i / d theta.  This is
+ * CustomSolver.backward with OursCUDA / Ours3D (wos/solver.py:109-114,
+ * wos/wos_grad.py:130-151, wos/wos_grad_3d.py:391-411) plus the gathers the
+ * forward attaches (wos/scene.py:353-357, wos/wos_with_source.py:89-90).
+ * Walks are recomputed from their Philox counters (same seed as the forward
+ * solve gives common random numbers).  Outputs are float32 device arrays that
+ * are ADDED to; any may be NULL when the matching want_* is 0. */
+WOS_API int wos_adjoint(wos_scene_t scene, const float *P, int n, const wos_params *p, const wos_adjoint_params *a,
+                const float *dLdu, float *dV, float *dg, float *dsrc, void *workspace, size_t workspace_bytes,
+                wos_stream_t stream);
+
+/* ---------------------------------------------------------------- kernels */
+
+/* Launch shape of the persistent walk kernels: threads per block, blocks per
+ * SM (0 = occupancy limit), walks taken per queue grab, LBVH nodes staged in
+ * shared memory per block.  In wos_set_launch_config, block_threads = 0,
+ * chunk = 0, blocks_per_sm < 0 and smem_nodes < 0 keep the current value. */
+typedef struct wos_launch_config {
+    int32_t block_threads;
+    int32_t blocks_per_sm;
+    int32_t chunk;
+    int32_t smem_nodes;
+} wos_launch_config;
+
+WOS_API int wos_set_launch_config(int dim, const wos_launch_config *cfg);
+WOS_API int wos_get_launch_config(int dim, wos_launch_config *out);
+
+/* Reference-style walk kernel: one thread per (point, walk), no walk
+ * regeneration, no shared-memory staging -- the shape of the reference's
+ * thrust::for_each launch (include/wos.cuh:407-440).  Same values as
+ * wos_walk_values; kept as the comparison kernel. */
+WOS_API int wos_walk_values_plain(wos_scene_t scene, const float *P, int n, const wos_params *p, float *values,
+                          wos_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WOS_B200_H */
