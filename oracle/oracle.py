@@ -101,6 +101,10 @@ def lib() -> ctypes.CDLL:
         L.orc_adjoint.argtypes = [P, P, I, ctypes.POINTER(Params), ctypes.POINTER(AdjParams), P, P, P, P, I]
         L.orc_math.argtypes = [I, P, P, P, I]
         L.orc_philox.argtypes = [ctypes.c_uint64, P, P, I]
+        L.orc_tri_closest.argtypes = [P, P, P, P, I, P, P]
+        L.orc_walk_counted.argtypes = [P, P, I, ctypes.POINTER(Params), P, I, P]
+        L.orc_adjoint_counted.argtypes = [P, P, I, ctypes.POINTER(Params), ctypes.POINTER(AdjParams), P, P, P, P, I,
+                                          P]
         _lib = L
     return _lib
 
@@ -174,7 +178,7 @@ class OracleScene:
         valid = np.ascontiguousarray(valid, np.uint8)
         pt, nrm = _f32(pt), _f32(nrm)
         R = np.zeros(valid.shape[0], np.float32)
-        lib().orc_inscribed_ball(self.h, _p(valid), _p(pt), _p(nrm), valid.shape[0], eps, int(use_bvh), _p(R),
+        lib().orc_inscribed_ball(self.h, _p(pt), _p(nrm), _p(valid), valid.shape[0], eps, int(use_bvh), _p(R),
                                  nthreads)
         return R
 
@@ -216,6 +220,27 @@ class OracleScene:
         return dV, dg, ds
 
 
+    def walk_counted(self, P, params: Params, nthreads=0):
+        """Per-walk values plus LBVH work totals {queries, node visits, prims}."""
+        P = _f32(P)
+        n = P.shape[0]
+        vals = np.zeros((n, params.nwalks), np.float32)
+        counts = np.zeros(3, np.int64)
+        lib().orc_walk_counted(self.h, _p(P), n, ctypes.byref(params), _p(vals), nthreads, _p(counts))
+        return vals, dict(queries=int(counts[0]), nodes=int(counts[1]), prims=int(counts[2]))
+
+    def adjoint_counted(self, P, params: Params, adj: AdjParams, dLdu, nthreads=0):
+        P = _f32(P)
+        dLdu = _f32(dLdu)
+        dV = np.zeros(self.V.shape, np.float64)
+        dg = np.zeros(self.V.shape[0], np.float64)
+        ds = np.zeros(5, np.float64)
+        counts = np.zeros(3, np.int64)
+        lib().orc_adjoint_counted(self.h, _p(P), P.shape[0], ctypes.byref(params), ctypes.byref(adj), _p(dLdu),
+                                  _p(dV), _p(dg), _p(ds), nthreads, _p(counts))
+        return (dV, dg, ds), dict(queries=int(counts[0]), nodes=int(counts[1]), prims=int(counts[2]))
+
+
 def reduce(vals):
     vals = _f32(vals)
     n, nw = vals.shape
@@ -238,6 +263,16 @@ def math_fn(which: str, x, y=None):
     out = np.zeros(x.shape[0] * (2 if which == "sincos_2pi" else 1), np.float32)
     lib().orc_math(codes[which], _p(x), _p(y), _p(out), x.shape[0])
     return out.reshape(-1, 2) if which == "sincos_2pi" else out
+
+
+def tri_closest(A, B, C, P):
+    """(uv = (w_b, w_c), distance) of points P to triangles (A, B, C)."""
+    A, B, C, P = _f32(A), _f32(B), _f32(C), _f32(P)
+    n = P.shape[0]
+    uv = np.zeros((n, 2), np.float32)
+    d = np.zeros(n, np.float32)
+    lib().orc_tri_closest(_p(A), _p(B), _p(C), _p(P), n, _p(uv), _p(d))
+    return uv, d
 
 
 def philox(seed: int, ctr):

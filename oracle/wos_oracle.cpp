@@ -369,10 +369,8 @@ static inline float seg_d2(const Scene &S, int f, const float *p, float *h_out) 
 // Closest point on triangle f (Ericson's Voronoi-region walk), written with
 // the precomputed products |ab|^2, ab.ac, |ac|^2.  Returns squared distance;
 // (v, w) are the barycentric weights of b and c; diff = x - closest point.
-static inline float tri_closest(const Scene &S, int f, const float *x, float *v_out, float *w_out,
-                                float *diff) {
-    const int *I = &S.F[(size_t)f * 3];
-    const float *a = &S.V[3 * I[0]], *b = &S.V[3 * I[1]], *c = &S.V[3 * I[2]];
+static inline float tri_closest_raw(const float *a, const float *b, const float *c, const float *x, float *v_out,
+                                    float *w_out, float *diff) {
     float ab[3], ac[3], ax[3];
     for (int k = 0; k < 3; ++k) {
         ab[k] = b[k] - a[k];
@@ -436,6 +434,11 @@ static inline float tri_closest(const Scene &S, int f, const float *x, float *v_
     return dot3(dd, dd);
 }
 
+static inline float tri_closest(const Scene &S, int f, const float *x, float *v_out, float *w_out, float *diff) {
+    const int *I = &S.F[(size_t)f * 3];
+    return tri_closest_raw(&S.V[3 * I[0]], &S.V[3 * I[1]], &S.V[3 * I[2]], x, v_out, w_out, diff);
+}
+
 static inline float prim_d2(const Scene &S, int f, const float *p) {
     return S.D == 2 ? seg_d2(S, f, p, nullptr) : tri_closest(S, f, p, nullptr, nullptr, nullptr);
 }
@@ -477,6 +480,10 @@ static inline float prune_tol2(const Scene &S, const float *p) {
     return 1025.0f * (e * e);
 }
 static inline float prune_bound(float best, float tol2) { return fmaf(best, 1.0009765625f, tol2); }
+
+// Per-thread traversal counters (node visits, primitive tests, queries) for
+// the algorithmic-work figures of the benchmark.
+static thread_local long long t_nbox = 0, t_nprim = 0, t_nquery = 0;
 
 // LBVH nearest (replaces lbvh::query_device, include/scene.cuh:130-146):
 // nearest-first descent, conservative pruning, ties to the lowest index.
@@ -530,6 +537,9 @@ static Hit nearest_bvh(const Scene &S, const float *p, int *nbox, int *nprim) {
     }
     if (nbox) *nbox = cb;
     if (nprim) *nprim = cp;
+    t_nbox += cb;
+    t_nprim += cp;
+    t_nquery += 1;
     return h;
 }
 
@@ -1243,6 +1253,48 @@ void orc_adjoint(void *s, const float *P, int n, const Params *prm, const AdjPar
     }
 }
 
+// Totals of the traversal counters over all threads of the last
+// orc_adjoint_counted / orc_walk_counted call: {queries, node visits, prims}.
+static long long g_counts[3] = {0, 0, 0};
+
+static void count_begin() {
+#pragma omp parallel
+    {
+        t_nbox = 0;
+        t_nprim = 0;
+        t_nquery = 0;
+    }
+}
+static void count_end() {
+    long long a = 0, b = 0, c = 0;
+#pragma omp parallel reduction(+ : a, b, c)
+    {
+        a += t_nquery;
+        b += t_nbox;
+        c += t_nprim;
+    }
+    g_counts[0] = a;
+    g_counts[1] = b;
+    g_counts[2] = c;
+}
+
+void orc_walk_counted(void *s, const float *P, int n, const Params *prm, float *vals, int nthreads, long long *counts) {
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    count_begin();
+    orc_walk_values(s, P, n, prm, vals, nullptr, nullptr, nthreads);
+    count_end();
+    for (int k = 0; k < 3; ++k) counts[k] = g_counts[k];
+}
+
+void orc_adjoint_counted(void *s, const float *P, int n, const Params *prm, const AdjParams *ap, const float *dLdu,
+                         double *dV, double *dg, double *dsrc, int nthreads, long long *counts) {
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    count_begin();
+    orc_adjoint(s, P, n, prm, ap, dLdu, dV, dg, dsrc, nthreads);
+    count_end();
+    for (int k = 0; k < 3; ++k) counts[k] = g_counts[k];
+}
+
 // Test hooks for the elementary functions.
 void orc_math(int which, const float *x, const float *y, float *out, int n) {
     for (int i = 0; i < n; ++i) {
@@ -1260,6 +1312,17 @@ void orc_math(int which, const float *x, const float *y, float *out, int n) {
             case 4: out[i] = wosm::exp_(x[i]); break;
             case 5: out[i] = wosm::atan2_(x[i], y[i]); break;
         }
+    }
+}
+
+// Point-triangle closest point on raw triangles: uv = (w_b, w_c), distance.
+void orc_tri_closest(const float *A, const float *B, const float *C, const float *P, int n, float *uv, float *d) {
+    for (int i = 0; i < n; ++i) {
+        float v, w;
+        const float d2 = tri_closest_raw(&A[3 * i], &B[3 * i], &C[3 * i], &P[3 * i], &v, &w, nullptr);
+        uv[2 * i] = v;
+        uv[2 * i + 1] = w;
+        d[i] = sqrtf(d2);
     }
 }
 
