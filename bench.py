@@ -1,0 +1,473 @@
+#!/usr/bin/env python
+"""Benchmark of the walk-on-spheres hot path on B200.
+
+Workload (one "step", the 2D differentiable solve): star polyline
+r(theta) = 0.6 + 0.25 cos(5 theta) with 4096 CCW segments, Dirichlet data
+g = sin(3x) cos(2y) at the vertices, constant source f = 1 (source type 2,
+amplitude 0, offset 1) sampled with the tabulated Green's-function CDF,
+queries = the 512 x 512 grid on [-1, 1]^2 masked to the interior (80,222
+points), 256 walks per point, nsteps 64, epsilon 1e-3.  A step is the
+forward solve (per-point means) followed by the adjoint of loss = mean(u^2)
+with respect to per-vertex g, the source parameters and the vertex positions
+(boundary-shape estimator, epsilon2 1e-3, clamping 0.1).  All inputs are
+seeded synthetic data of these shapes.
+
+value   walks/s of whole steps on the device (inputs resident in HBM), summed
+        over all ranks; each walk is both a forward walk and an adjoint sample.
+e2e     the same metric through the public Python API (wos.CustomSolver with
+        WoSWithSourceCUDA forward and OursCUDA backward, torch autograd) with
+        host buffers: H2D of points and scene, scene build, forward, backward,
+        D2H of loss and gradients inside the timed region.
+roofline  the adjoint kernel (the dominant one): algorithmic bytes per launch
+        (32 B per LBVH node visit + 16 B per segment test, counted on the
+        device for this exact launch) / its CUDA-event time, against the
+        measured HBM copy bandwidth.  `issue` gives FP32 algorithmic ops
+        (12 per node visit, 20 per segment test, 10 per query) against
+        148 SMs x 128 lanes x 2 x SM clock.
+--impl reference  the CPU restatement of the reference algorithm (the
+        reference itself cannot run: it needs Dr.Jit/Mitsuba and the lbvh
+        submodule), all host threads, bounded samples of the same workload.
+
+Multi-GPU (torchrun): every rank runs the same workload with its own seed on
+its own GPU (weak scaling, no data-path collective); times are the max over
+ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "diff-wos_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "wos_walks_per_s"
+UNIT = "walks/s"
+STAR = dict(n=4096, r0=0.6, amp=0.25, lobes=5)
+GRID = 512
+NWALKS = 256
+NSTEPS = 64
+EPS = 1e-3
+EPS2 = 1e-3
+CLAMP = 0.1
+SOURCE = [0.0, 0.0, 0.0, 0.0, 1.0]
+
+
+# ---------------------------------------------------------------- workload
+def set_size(grid, walks):
+    global GRID, NWALKS
+    GRID, NWALKS = int(grid), int(walks)
+
+
+def make_workload():
+    from wos import shapes
+    V, F = shapes.star(STAR["n"], STAR["r0"], STAR["amp"], STAR["lobes"])
+    g = (np.sin(3 * V[:, 0]) * np.cos(2 * V[:, 1])).astype(np.float32)
+    P = shapes.grid(GRID, -1.0, 1.0)
+    P = P[shapes.inside_star(P, STAR["r0"], STAR["amp"], STAR["lobes"])]
+    return V, F, g, np.ascontiguousarray(P)
+
+
+def walk_settings(seed):
+    from wos.native import WalkSettings
+    return WalkSettings(nwalks=NWALKS, nsteps=NSTEPS, epsilon=EPS, use_IS_for_greens=True, include_source=True,
+                        use_bvh=True, seed=seed)
+
+
+def adjoint_settings():
+    from wos.native import AdjointSettings
+    return AdjointSettings(epsilon2=EPS2, clamping=CLAMP, control_variates=True, source_in_normal_derivative=True,
+                           want_dV=True, want_dg=True, want_dsrc=True)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples every 200 ms during the timed region."""
+
+    QUERY = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        rows = [l.split(", ") for l in self.lines if l]
+        if self.uuid:
+            mine = [r for r in rows if len(r) > 1 and self.uuid in r[1]]
+            rows = mine or rows
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[2]))
+                mx.append(float(r[3]))
+            except (ValueError, IndexError):
+                continue
+            for name, v in zip(names, r[6:10]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- measured peaks
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- CPU baseline
+def cpu_baseline(V, F, g, P, target_s=6.0, seed=0):
+    """The oracle (C++ restatement of the reference walk, OpenMP, all host
+    threads) on a bounded sample of the same step: forward walks + adjoint
+    samples at NWALKS walks per point."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as O
+    S = O.OracleScene(V, F, g, 2, SOURCE)
+    prm = O.make_params(nwalks=NWALKS, nsteps=NSTEPS, epsilon=EPS, use_IS_for_greens=True, include_source=True,
+                        use_bvh=True, seed=seed)
+    adj = O.make_adj(EPS2, CLAMP, True, True, 1e-3, True, True, True)
+    threads = os.cpu_count() or 1
+
+    def run(n):
+        idx = np.linspace(0, len(P) - 1, n).astype(np.int64)
+        sub = P[idx]
+        t0 = time.perf_counter()
+        vals, _, _ = S.walk_values(sub, prm, nthreads=threads)
+        mean, _ = O.reduce(vals)
+        dLdu = (2.0 * mean / len(P)).astype(np.float32)
+        S.adjoint(sub, prm, adj, dLdu, nthreads=threads)
+        return time.perf_counter() - t0
+
+    probe = 8
+    t = run(probe)
+    n = int(max(probe, min(len(P), probe * target_s / max(t, 1e-3))))
+    return S, prm, adj, run, n, threads
+
+
+def cpu_info():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    V, F, g, P = make_workload()
+    S, prm, adj, run, n, threads = cpu_baseline(V, F, g, P, target_s=args.ref_step_s)
+    for _ in range(args.warmup):
+        run(n)
+    ts = [run(n) for _ in range(args.steps)]
+    t = float(np.mean(ts))
+    value = n * NWALKS / t
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(len(P), per_step_points=n),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{n} of {len(P)} points x {NWALKS} walks (forward + adjoint), oracle C++ "
+                                   f"restatement, {threads} threads, {cpu_info()}"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference needs Dr.Jit/Mitsuba and its lbvh submodule and cannot run; "
+                "its algorithm is timed through the C++ restatement",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(npts, per_step_points=None):
+    c = {"workload": f"2d_differentiable_solve_star4096_grid{GRID}_walks{NWALKS}",
+         "scene": "star r=0.6+0.25cos(5t), 4096 segments", "points": npts, "walks_per_point": NWALKS,
+         "nsteps": NSTEPS, "epsilon": EPS, "epsilon2": EPS2, "source": "f=1, G-CDF importance sampling",
+         "loss": "mean(u^2); adjoint wrt g, f, vertex xy", "nearest": "LBVH",
+         "l2": "inputs < L2; 256 MiB buffer written between timed steps (L2 flush)"}
+    if per_step_points is not None:
+        c["points_per_step"] = per_step_points
+    return c
+
+
+# ---------------------------------------------------------------- GPU arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ref-step-s", type=float, default=6.0)
+    ap.add_argument("--grid", type=int, default=GRID, help="query grid (smaller only for profiling captures)")
+    ap.add_argument("--walks", type=int, default=NWALKS, help="walks per point (smaller only for profiling)")
+    args = ap.parse_args()
+    set_size(args.grid, args.walks)
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return reference_arm(args, world, rank)
+
+    import torch
+    import torch.distributed as dist
+    import wos
+    from wos.native import NativeScene
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    V, F, g, P = make_workload()
+    n = len(P)
+    dev = torch.device("cuda", local)
+    scene = NativeScene(V, F, g, 2, SOURCE)
+    P_d = torch.as_tensor(P, device=dev)
+    ws = walk_settings(seed=1000 * rank)
+    adj = adjoint_settings()
+    solve_ws = torch.empty(0, dtype=torch.uint8, device=dev)
+    adj_ws = torch.empty(0, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def step(seed, times=None):
+        s = walk_settings(seed)
+        e0, e1, e2 = ev(), ev(), ev()
+        e0.record(stream)
+        mean = scene.solve(P_d, s, workspace=solve_ws_holder[0])
+        e1.record(stream)
+        dLdu = (2.0 / n) * mean.to(torch.float32)
+        out = scene.adjoint(P_d, s, adj, dLdu, workspace=adj_ws_holder[0])
+        e2.record(stream)
+        if times is not None:
+            times.append((e0, e1, e2))
+        return mean, out
+
+    import ctypes
+    from wos import _lib
+    c = ws.c()
+    solve_ws_holder = [torch.empty(_lib.lib().wos_solve_workspace_size(n, ctypes.byref(c)), dtype=torch.uint8,
+                                   device=dev)]
+    adj_ws_holder = [torch.empty(_lib.lib().wos_adjoint_workspace_size(scene.h), dtype=torch.uint8, device=dev)]
+
+    # -- work counting pass (untimed): exact LBVH work of one step's launches
+    wos.set_work_counting(True)
+    _lib.work_counters(reset=True)
+    s0 = walk_settings(7)
+    mean0 = scene.solve(P_d, s0, workspace=solve_ws_holder[0])
+    torch.cuda.synchronize()
+    fwd_work = _lib.work_counters(reset=True)
+    scene.adjoint(P_d, s0, adj, (2.0 / n) * mean0.to(torch.float32), workspace=adj_ws_holder[0])
+    torch.cuda.synchronize()
+    adj_work = _lib.work_counters(reset=True)
+    wos.set_work_counting(False)
+
+    # -- warm-up
+    for w in range(args.warmup):
+        step(10_000 + w)
+    torch.cuda.synchronize()
+    wos.device_status(reset=True)
+
+    # -- timed steps (device), L2 flushed between steps
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    times = []
+    for k in range(args.steps):
+        flush.zero_()
+        step(1000 * rank + k, times)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    t_solve = [a.elapsed_time(b) * 1e-3 for a, b, _ in times]
+    t_adj = [b.elapsed_time(c) * 1e-3 for _, b, c in times]
+    t_step = float(np.sum(t_solve) + np.sum(t_adj))
+    t_max = max_over_ranks(t_step)
+    status = wos.device_status(reset=False)
+
+    total_walks = world * n * NWALKS * args.steps
+    value = total_walks / t_max
+    ms_per_step = t_max / args.steps * 1e3
+
+    # -- e2e through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = e2e_bench(args, V, F, g, P, rank, world, dev, max_over_ranks, barrier)
+
+    # -- plain (reference-shaped) forward kernel vs the persistent one, same walks
+    plain = plain_vs_persistent(scene, P_d, n)
+
+    # -- roofline of the adjoint kernel
+    hbm, peak_kind = peaks()
+    adj_avg = float(np.mean(t_adj))
+    adj_bytes = 32.0 * adj_work["nodes"] + 16.0 * adj_work["prims"]
+    adj_flops = 12.0 * adj_work["nodes"] + 20.0 * adj_work["prims"] + 10.0 * adj_work["queries"]
+    achieved = adj_bytes / adj_avg / 1e9
+    sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6
+    traffic = None
+    tp = ROOT / "profiles" / "roofline_traffic.json"
+    if tp.exists():
+        tj = json.load(open(tp))
+        if tj.get("kernel") == "k_adjoint" and tj.get("workload") == workload_config(n)["workload"]:
+            traffic = tj.get("traffic_bytes_per_launch")
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(n),
+        "adjoint_pts_per_s": world * n * args.steps / t_max,
+        "breakdown_ms": {"forward": float(np.mean(t_solve)) * 1e3, "adjoint": adj_avg * 1e3},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic, "kernel": "k_adjoint", "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": adj_bytes,
+                     "work_per_launch": adj_work, "forward_work_per_launch": fwd_work,
+                     "issue": {"achieved_tflops": adj_flops / adj_avg / 1e12, "peak_tflops": fp32_peak / 1e12,
+                               "frac": adj_flops / adj_avg / fp32_peak}},
+        "gpu_launches": args.steps * 6,
+        "device_status": status,
+        "plain_vs_persistent": plain,
+    }
+    if clk is not None:
+        line["clocks"] = clk
+    if e2e is not None:
+        line["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        S, prm, adjp, run, m, threads = cpu_baseline(V, F, g, P)
+        ts = [run(m) for _ in range(2)]
+        tcpu = float(np.mean(ts))
+        line["cpu_baseline"] = {"value": m * NWALKS / tcpu, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{m} of {n} points x {NWALKS} walks (forward + adjoint), "
+                                          f"{threads} threads, {cpu_info()}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def plain_vs_persistent(scene, P_d, n):
+    """Forward-only walks/s of the reference-shaped kernel (one thread per
+    walk, no regeneration) and of the persistent kernel, same walks."""
+    import torch
+    s = walk_settings(3)
+    out = {}
+    for name, plain in (("plain", True), ("persistent", False)):
+        scene.values(P_d, s, plain=plain)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        scene.values(P_d, s, plain=plain)
+        b.record()
+        torch.cuda.synchronize()
+        out[name + "_fwd_walks_per_s"] = n * NWALKS / (a.elapsed_time(b) * 1e-3)
+    return out
+
+
+def e2e_bench(args, V, F, g, P, rank, world, dev, max_over_ranks, barrier):
+    import torch
+    import wos
+    Vh = torch.from_numpy(V).pin_memory()
+    Fh = torch.from_numpy(F).pin_memory()
+    gh = torch.from_numpy(g).pin_memory()
+    Ph = torch.from_numpy(P).pin_memory()
+    sh = torch.tensor(SOURCE, dtype=torch.float32).pin_memory()
+    n = len(P)
+    fwd = wos.WoSWithSourceCUDA(nwalks=NWALKS, nsteps=NSTEPS, epsilon=EPS, use_IS_for_greens=True)
+    bwd = wos.OursCUDA(nwalks=NWALKS, nsteps=NSTEPS, epsilon=EPS, epsilon2=EPS2, clamping=CLAMP, grad_values=True,
+                       grad_source=True, use_IS_for_greens=True)
+    solver = wos.CustomSolver(fwd_solver=fwd, bwd_solver=bwd)
+    h2d = Vh.numel() * 4 + Fh.numel() * 4 + gh.numel() * 4 + Ph.numel() * 4 + sh.numel() * 4
+    d2h = 4 + Vh.numel() * 4 + gh.numel() * 4 + sh.numel() * 4
+
+    def one(seed):
+        Vd = Vh.to(dev, non_blocking=True).requires_grad_(True)
+        gd = gh.to(dev, non_blocking=True).requires_grad_(True)
+        sd = sh.to(dev, non_blocking=True).requires_grad_(True)
+        Pd = Ph.to(dev, non_blocking=True)
+        scene = wos.Polyline(Vd, Fh.to(dev, non_blocking=True), gd, source_type=2, source_params=sd, use_bvh=True)
+        u = solver.walk(Pd, scene, seed=seed)
+        loss = (u * u).mean()
+        loss.backward()
+        return loss.detach().cpu(), Vd.grad.cpu(), gd.grad.cpu(), sd.grad.cpu()
+
+    for w in range(args.warmup):
+        one(20_000 + w)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(args.steps):
+        one(30_000 + 1000 * rank + k)
+    e1.record()
+    torch.cuda.synchronize()
+    t = max_over_ranks(e0.elapsed_time(e1) * 1e-3)
+    return {"value": world * n * NWALKS * args.steps / t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": t / args.steps * 1e3,
+            "path": "wos.CustomSolver(WoSWithSourceCUDA, OursCUDA).walk + torch autograd, pinned host buffers"}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -395,6 +395,16 @@ int wos_adjoint(wos_scene_t scene, const float *P, int n, const wos_params *p, c
     return 0;
 }
 
+int wos_set_work_counting(int enable) { return set_work_counting(enable); }
+
+int wos_work_counters(int reset, int64_t *out) {
+    if (out == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "out is NULL");
+    unsigned long long v[3] = {0, 0, 0};
+    const int rc = read_work(reset, v);
+    for (int k = 0; k < 3; ++k) out[k] = (int64_t)v[k];
+    return rc;
+}
+
 int wos_set_launch_config(int dim, const wos_launch_config *cfg) {
     if (cfg == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "cfg is NULL");
     return set_launch_config(dim, cfg);

@@ -25,6 +25,7 @@
 namespace wosd {
 
 __device__ int g_status;
+__device__ unsigned long long g_work[3];
 
 int read_status(int reset, int *out) {
     int v = 0;
@@ -39,10 +40,32 @@ int read_status(int reset, int *out) {
     return 0;
 }
 
+int read_work(int reset, unsigned long long *out) {
+    cudaError_t e = cudaMemcpyFromSymbol(out, g_work, sizeof(unsigned long long) * 3);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpyFromSymbol(g_work)");
+    if (reset) {
+        const unsigned long long z[3] = {0, 0, 0};
+        e = cudaMemcpyToSymbol(g_work, z, sizeof(z));
+        if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpyToSymbol(g_work)");
+    }
+    return 0;
+}
+
 template <int D, bool BVH>
-__device__ __forceinline__ Hit query(const SceneView &S, const float *p, const float4 *top, int n_top) {
-    if (BVH) return nearest_bvh<D>(S, p, top, n_top, &g_status);
-    return nearest_brute<D>(S, p);
+__device__ __forceinline__ Hit query(const SceneView &S, const float *p, const float4 *top, int n_top, Work &wk) {
+    if (BVH) return nearest_bvh<D>(S, p, top, n_top, &g_status, wk);
+    return nearest_brute<D>(S, p, wk);
+}
+
+// Add a warp's work counters to the global totals (counting launches only).
+__device__ __forceinline__ void flush_work(const Work &wk) {
+    unsigned long long v[3] = {wk.nq, wk.nb, wk.np};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&g_work[k], v[k]);
+    }
 }
 
 // ------------------------------------------------------------------ walker
@@ -184,6 +207,7 @@ __global__ void __launch_bounds__(512) k_walk(SceneView S, WalkCfg c, const floa
     long long idx = 0;
     uint32_t pt = 0, wk = 0;
     Walker w;
+    Work work{0, 0, 0};
     for (;;) {
         const bool was = active;
         if (!refill(q, active, idx, counter, total, chunk)) break;
@@ -198,7 +222,7 @@ __global__ void __launch_bounds__(512) k_walk(SceneView S, WalkCfg c, const floa
             w.start(P + (size_t)pt * D, D);
         }
         if (!active) continue;
-        const Hit hit = query<D, BVH>(S, w.p, top, n_top);
+        const Hit hit = query<D, BVH>(S, w.p, top, n_top, work);
         const int r = walker_advance<D>(w, S, hit, c, c.eps, c.project != 0, c.prevent_fd != 0, pt, wk, ROLE_PRIMAL,
                                         false, cdf);
         if (r == W_CONTINUE) continue;
@@ -231,6 +255,7 @@ __global__ void __launch_bounds__(512) k_walk(SceneView S, WalkCfg c, const floa
             if (out.steps) out.steps[idx] = r == W_TRUNC ? c.nsteps : w.i;
         }
     }
+    if (c.count) flush_work(work);
 }
 
 // Reference-shaped kernel: one thread per (point, walk), no regeneration.
@@ -243,9 +268,10 @@ __global__ void __launch_bounds__(256) k_walk_plain(SceneView S, WalkCfg c, cons
     const uint32_t wk = c.walk_offset + (uint32_t)(idx - (long long)pt * c.nwalks);
     Walker w;
     w.start(P + (size_t)pt * D, D);
+    Work work{0, 0, 0};
     float v = 0.0f;
     for (;;) {
-        const Hit hit = query<D, BVH>(S, w.p, nullptr, 0);
+        const Hit hit = query<D, BVH>(S, w.p, nullptr, 0, work);
         const int r = walker_advance<D>(w, S, hit, c, c.eps, c.project != 0, c.prevent_fd != 0, pt, wk, ROLE_PRIMAL,
                                         false, S.cdf);
         if (r == W_CONTINUE) continue;
@@ -304,7 +330,8 @@ __global__ void k_closest(SceneView S, const float *__restrict__ P, int n, Query
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float p[3] = {P[(size_t)i * D], P[(size_t)i * D + 1], D == 3 ? P[(size_t)i * D + 2] : 0.0f};
-    const Hit hit = query<D, BVH>(S, p, nullptr, 0);
+    Work work{0, 0, 0};
+    const Hit hit = query<D, BVH>(S, p, nullptr, 0, work);
     if (o.prim) o.prim[i] = hit.prim;
     if (o.dist) o.dist[i] = sqrtf(hit.d2);
     if (hit.prim < 0) {
@@ -334,12 +361,13 @@ template <int D, bool BVH>
 __device__ __forceinline__ float inscribed_ball(const SceneView &S, const float *p, const float *n, float eps,
                                                 const float4 *top, int n_top) {
     float b = S.half_min_extent, a = eps;
+    Work work{0, 0, 0};
     for (int i = 0; i < 10; ++i) {
         const float m = (a + b) * 0.5f;
         float q[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
         for (int k = 0; k < D; ++k) q[k] = fmaf(n[k], m, p[k]);
-        const float d = sqrtf(query<D, BVH>(S, q, top, n_top).d2);
+        const float d = sqrtf(query<D, BVH>(S, q, top, n_top, work).d2);
         if (fabsf(d - m) < 1e-5f)
             a = m;
         else
@@ -536,6 +564,7 @@ __global__ void __launch_bounds__(512) k_adjoint(SceneView S, WalkCfg c, AdjCfg 
     float ba = 0.0f, bb = 0.0f;
     int bk = 0;
     double acc_src[5] = {0, 0, 0, 0, 0};
+    Work work{0, 0, 0};
 
     for (;;) {
         const bool was = active;
@@ -584,7 +613,7 @@ __global__ void __launch_bounds__(512) k_adjoint(SceneView S, WalkCfg c, AdjCfg 
             phase = PH_BALL;
         }
         const float *x = (phase == PH_PRIMAL || phase == PH_ANTI_WALK) ? w.p : qpos;
-        const Hit hit = query<D, BVH>(S, x, top, n_top);
+        const Hit hit = query<D, BVH>(S, x, top, n_top, work);
         bool finish_anti = false;
         float uq = 0.0f;
         if (phase == PH_PRIMAL) {
@@ -711,6 +740,7 @@ __global__ void __launch_bounds__(512) k_adjoint(SceneView S, WalkCfg c, AdjCfg 
             phase = PH_IDLE;
         }
     }
+    if (c.count) flush_work(work);
     if (want_src) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
@@ -753,8 +783,16 @@ int get_launch_config(int dim, wos_launch_config *out) {
     return 0;
 }
 
+static int g_count_work = 0;
+
+int set_work_counting(int enable) {
+    g_count_work = enable ? 1 : 0;
+    return 0;
+}
+
 WalkCfg make_cfg(const wos_params &p) {
     WalkCfg c;
+    c.count = g_count_work;
     c.nwalks = p.nwalks;
     c.nsteps = p.nsteps;
     c.eps = p.epsilon;

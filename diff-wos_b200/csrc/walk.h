@@ -16,6 +16,7 @@ struct WalkCfg {
     int double_sided, prevent_fd, use_IS, include_source, project;
     uint32_t walk_offset;
     Rng rng;
+    int count;  // accumulate LBVH work counters (wos_set_work_counting)
 };
 
 // Device copy of wos_adjoint_params.
@@ -52,6 +53,8 @@ struct AdjOut {
 
 WalkCfg make_cfg(const wos_params &p);
 int read_status(int reset, int *out);
+int read_work(int reset, unsigned long long *out);
+int set_work_counting(int enable);
 int set_launch_config(int dim, const wos_launch_config *cfg);
 int get_launch_config(int dim, wos_launch_config *out);
 

@@ -193,6 +193,12 @@ struct Hit {
     float d2;
 };
 
+// Per-thread LBVH work counters: queries, node visits (two child boxes each),
+// primitive distance evaluations.
+struct Work {
+    unsigned nq, nb, np;
+};
+
 // Pruning slack (same rule as the oracle): a box is skipped only when its
 // squared distance exceeds (1 + 2^-10) best + 1025 (s 2^-20)^2, where s
 // bounds the coordinates' magnitude around the scene.
@@ -211,8 +217,10 @@ __device__ __forceinline__ float prune_bound(float best, float tol2) { return fm
 // Brute-force nearest over the original primitive order, ties to the lowest
 // index (include/scene.cuh:102-128).
 template <int D>
-__device__ __forceinline__ Hit nearest_brute(const SceneView &S, const float *p) {
+__device__ __forceinline__ Hit nearest_brute(const SceneView &S, const float *p, Work &wk) {
     Hit h{-1, INFINITY};
+    wk.nq += 1;
+    wk.np += (unsigned)S.nF;
     if (D == 2) {
         for (int f = 0; f < S.nF; ++f) {
             float t;
@@ -286,9 +294,11 @@ __device__ __forceinline__ void load_node(const float4 *base, int k, float (*lo)
 // shallowest, breadth-first) are read from shared memory.
 template <int D>
 __device__ __forceinline__ Hit nearest_bvh(const SceneView &S, const float *p, const float4 *top, int n_top,
-                                           int *status) {
+                                           int *status, Work &wk) {
     Hit h{-1, INFINITY};
+    wk.nq += 1;
     if (S.nF == 1) {
+        wk.np += 1;
         h.prim = 0;
         if (D == 2) {
             float t;
@@ -309,6 +319,7 @@ __device__ __forceinline__ Hit nearest_bvh(const SceneView &S, const float *p, c
         --sp;
         const int v = stn[sp];
         if (std2[sp] > prune_bound(h.d2, tol2)) continue;
+        wk.nb += 1;
         float lo[2][3], hi[2][3];
         int ch[2];
         if (v < n_top)
@@ -327,6 +338,7 @@ __device__ __forceinline__ Hit nearest_bvh(const SceneView &S, const float *p, c
             const float bdc = pass == 0 ? dn : df;
             if (c < 0 && bdc <= prune_bound(h.d2, tol2)) {
                 const int leaf = ~c;
+                wk.np += 1;
                 float d2;
                 if (D == 2) {
                     float t;

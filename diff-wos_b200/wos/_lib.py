@@ -117,6 +117,8 @@ SIGNATURES = {
         _I,
         [_P, _P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams), _P, _P, _P, _P, _P, _S, _P],
     ),
+    "wos_set_work_counting": (_I, [_I]),
+    "wos_work_counters": (_I, [_I, ctypes.POINTER(ctypes.c_int64)]),
     "wos_set_launch_config": (_I, [_I, ctypes.POINTER(WosLaunchConfig)]),
     "wos_get_launch_config": (_I, [_I, ctypes.POINTER(WosLaunchConfig)]),
 }
@@ -153,6 +155,17 @@ def device_status(reset: bool = False) -> int:
     v = ctypes.c_int32(0)
     call("wos_device_status", int(reset), ctypes.byref(v))
     return int(v.value)
+
+
+def set_work_counting(enable: bool) -> None:
+    call("wos_set_work_counting", int(enable))
+
+
+def work_counters(reset: bool = False) -> dict:
+    """Totals since the last reset: {queries, nodes, prims}."""
+    v = (ctypes.c_int64 * 3)()
+    call("wos_work_counters", int(reset), v)
+    return dict(queries=int(v[0]), nodes=int(v[1]), prims=int(v[2]))
 
 
 def get_launch_config(dim: int) -> WosLaunchConfig:

@@ -238,6 +238,13 @@ typedef struct wos_launch_config {
     int32_t smem_nodes;
 } wos_launch_config;
 
+/* Work accounting: while enabled, the persistent walk and adjoint kernels add
+ * their nearest-query totals to a device counter {queries, LBVH node visits,
+ * primitive distance evaluations} (brute force: nF evaluations per query).
+ * wos_work_counters reads it (synchronising the device); reset != 0 clears. */
+WOS_API int wos_set_work_counting(int enable);
+WOS_API int wos_work_counters(int reset, int64_t *out);
+
 WOS_API int wos_set_launch_config(int dim, const wos_launch_config *cfg);
 WOS_API int wos_get_launch_config(int dim, wos_launch_config *out);
 

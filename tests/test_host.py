@@ -1,0 +1,130 @@
+"""Host-side logic that needs no GPU: synthetic workloads, OBJ I/O, solver
+settings (reference semantics of each solver class), the sampler."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+
+def test_c1_point_count():
+    from wos import shapes
+    P = shapes.grid(128, -0.9, 0.9)
+    assert len(P[np.hypot(P[:, 0], P[:, 1]) < 1.0]) == 14592
+
+
+def test_c2_point_count():
+    from wos import shapes
+    P = shapes.grid(512)
+    n = int(shapes.inside_star(P).sum())
+    assert abs(n - 80222) < 200
+
+
+def test_grid_flips_y():
+    from wos import shapes
+    P = shapes.grid(3)
+    assert P[0, 1] == 1.0 and P[-1, 1] == -1.0 and P[0, 0] == -1.0
+
+
+def test_icosphere_counts_and_orientation():
+    from wos import shapes
+    V, F = shapes.icosphere(6)
+    assert F.shape == (81920, 3) and V.shape == (40962, 3)
+    V, F = shapes.displaced_icosphere(3, 0.15, 0)
+    a, b, c = V[F[:, 0]], V[F[:, 1]], V[F[:, 2]]
+    n = np.cross(b - a, c - a)
+    assert np.all((n * (a + b + c)).sum(1) > 0)  # outward
+    # closed 2-manifold: every edge shared by exactly two faces
+    e = np.sort(np.concatenate([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]]]), 1)
+    _, counts = np.unique(e, axis=0, return_counts=True)
+    assert np.all(counts == 2)
+
+
+def test_circle_is_ccw():
+    from wos import shapes
+    V, F = shapes.circle(64)
+    area = 0.5 * np.sum(V[F[:, 0], 0] * V[F[:, 1], 1] - V[F[:, 1], 0] * V[F[:, 0], 1])
+    assert area > 0
+
+
+def test_value_noise_seeded():
+    from wos import shapes
+    P = np.random.default_rng(0).normal(size=(100, 3))
+    a = shapes.value_noise3(P, seed=1)
+    assert np.array_equal(a, shapes.value_noise3(P, seed=1))
+    assert not np.array_equal(a, shapes.value_noise3(P, seed=2))
+    assert np.abs(a).max() <= 1.0
+
+
+def test_obj_roundtrip(tmp_path):
+    from wos import io, shapes
+    V, F = shapes.circle(16)
+    g = np.arange(16, dtype=np.float32)
+    io.write_2d_obj(tmp_path / "c.obj", V, F, g)
+    V2, F2, g2 = io.read_2d_obj(tmp_path / "c.obj")
+    np.testing.assert_allclose(V2, V, atol=1e-6)
+    assert np.array_equal(F2, F) and np.array_equal(g2, g)
+    V2, F2, _ = io.read_2d_obj(tmp_path / "c.obj", flip_orientation=True)
+    assert np.array_equal(F2, F[:, ::-1])
+    T, TF = shapes.icosphere(1)
+    io.write_3d_obj(tmp_path / "s.obj", T, TF)
+    T2, TF2, g3 = io.read_3d_obj(tmp_path / "s.obj")
+    np.testing.assert_allclose(T2, T, atol=1e-6)
+    assert np.array_equal(TF2, TF) and len(g3) == 0
+
+
+class _FakeScene:
+    def __init__(self, dim=2, source_type=0, use_bvh=True):
+        self.dim = dim
+        self.source_type = source_type
+        self.use_bvh = use_bvh
+
+
+def test_solver_semantics_match_reference_classes():
+    import wos
+    s = _FakeScene(source_type=2)
+    # the Dr.Jit WoS projects unterminated walks; the CUDA walk marks them invalid
+    assert wos.WoS().walk_settings(s).project_unterminated is True
+    assert wos.WoSCUDA().walk_settings(s).project_unterminated is False
+    assert wos.WoS3D().walk_settings(_FakeScene(3)).project_unterminated is True
+    assert wos.WoS3DCUDA().walk_settings(_FakeScene(3)).project_unterminated is False
+    # defaults of the reference dataclasses
+    w = wos.WoS()
+    assert (w.epsilon, w.nwalks, w.nsteps) == (1e-3, 10, 32)
+    base = wos.Solver()
+    assert (base.epsilon, base.nwalks, base.nsteps) == (0.005, 20, 4)
+    # source term only for the with-source solvers
+    assert wos.WoSCUDA().walk_settings(s).include_source is False
+    assert wos.WoSWithSourceCUDA().walk_settings(s).include_source is True
+    assert wos.WoSWithSourceCUDA().walk_settings(_FakeScene(2, 0)).include_source is False
+    assert wos.WoSWithSourceCUDA(use_IS_for_greens=True).walk_settings(s).use_IS_for_greens is True
+    # gradients: values from every value solver, source only from the attached (Dr.Jit) variant
+    a = wos.WoSWithSource().adjoint_settings(s, True, True, True)
+    assert (a.want_dV, a.want_dg, a.want_dsrc) == (False, True, True)
+    a = wos.WoSWithSourceCUDA().adjoint_settings(s, True, True, True)
+    assert (a.want_dV, a.want_dg, a.want_dsrc) == (False, True, False)
+    a = wos.OursCUDA().adjoint_settings(s, True, True, True)
+    assert (a.want_dV, a.want_dg, a.want_dsrc) == (True, False, False)
+    a = wos.OursCUDA(grad_values=True, grad_source=True, epsilon2=5e-4).adjoint_settings(s, True, True, True)
+    assert (a.want_dV, a.want_dg, a.want_dsrc, a.epsilon2) == (True, True, True, 5e-4)
+
+
+def test_sampler_advances():
+    import wos
+    s = wos.Sampler(seed=5, offset=3)
+    assert s.take() == 3 and s.take() == 3 + 1 and s.offset == 5
+    from wos.solver import as_sampler
+    assert as_sampler(9).seed == 9 and as_sampler(s) is s
+
+
+def test_walk_settings_to_c():
+    from wos.native import WalkSettings
+    c = WalkSettings(nwalks=7, nsteps=9, epsilon=2e-3, seed=(1 << 63) + 5, walk_offset=(1 << 32) + 3).c()
+    assert (c.nwalks, c.nsteps, c.walk_offset, c.seed) == (7, 9, 3, (1 << 63) + 5)
+
+
+def test_statistics():
+    from wos import Statistics
+    x = np.random.default_rng(0).normal(size=1000)
+    st = Statistics()
+    assert np.isclose(st.mean(x)[-1], x.mean())
+    assert np.isclose(st.var(x)[-1], x.var())
