@@ -279,44 +279,47 @@ def main():
     P_d = torch.as_tensor(P, device=dev)
     ws = walk_settings(seed=1000 * rank)
     adj = adjoint_settings()
-    solve_ws = torch.empty(0, dtype=torch.uint8, device=dev)
-    adj_ws = torch.empty(0, dtype=torch.uint8, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
 
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
-
-    def step(seed, times=None):
-        s = walk_settings(seed)
-        e0, e1, e2 = ev(), ev(), ev()
-        e0.record(stream)
-        mean = scene.solve(P_d, s, workspace=solve_ws_holder[0])
-        e1.record(stream)
-        dLdu = (2.0 / n) * mean.to(torch.float32)
-        out = scene.adjoint(P_d, s, adj, dLdu, workspace=adj_ws_holder[0])
-        e2.record(stream)
-        if times is not None:
-            times.append((e0, e1, e2))
-        return mean, out
-
     import ctypes
     from wos import _lib
     c = ws.c()
-    solve_ws_holder = [torch.empty(_lib.lib().wos_solve_workspace_size(n, ctypes.byref(c)), dtype=torch.uint8,
-                                   device=dev)]
-    adj_ws_holder = [torch.empty(_lib.lib().wos_adjoint_workspace_size(scene.h), dtype=torch.uint8, device=dev)]
+    ca = adj.c()
+    fused_ws = torch.empty(_lib.lib().wos_solve_adjoint_workspace_size(scene.h, n, ctypes.byref(c), ctypes.byref(ca)),
+                           dtype=torch.uint8, device=dev)
+    solve_ws = torch.empty(_lib.lib().wos_solve_workspace_size(n, ctypes.byref(c)), dtype=torch.uint8, device=dev)
+    adj_ws = torch.empty(_lib.lib().wos_adjoint_workspace_size(scene.h), dtype=torch.uint8, device=dev)
 
-    # -- work counting pass (untimed): exact LBVH work of one step's launches
+    def step(seed):
+        """One fused forward + adjoint step (wos_solve_adjoint, loss = mean(u^2))."""
+        return scene.solve_adjoint(P_d, walk_settings(seed), adj, loss_kind=1, workspace=fused_ws)
+
+    def split_step(seed, times):
+        """The same kernels as separate calls, for the per-kernel breakdown."""
+        s = walk_settings(seed)
+        e0, e1, e2 = ev(), ev(), ev()
+        e0.record(stream)
+        mean, _, rec, dc = scene.solve_records(P_d, s, want_dcontrib=True, workspace=solve_ws)
+        e1.record(stream)
+        dLdu = (2.0 / n) * mean.to(torch.float32)
+        scene.adjoint_records(P_d, s, adj, dLdu, rec, dc, workspace=adj_ws)
+        e2.record(stream)
+        times.append((e0, e1, e2))
+
+    # -- work counting pass (untimed): exact tree work of one step's launches
     wos.set_work_counting(True)
     _lib.work_counters(reset=True)
     s0 = walk_settings(7)
-    mean0 = scene.solve(P_d, s0, workspace=solve_ws_holder[0])
+    mean0, _, rec0, dc0 = scene.solve_records(P_d, s0, want_dcontrib=True, workspace=solve_ws)
     torch.cuda.synchronize()
     fwd_work = _lib.work_counters(reset=True)
-    scene.adjoint(P_d, s0, adj, (2.0 / n) * mean0.to(torch.float32), workspace=adj_ws_holder[0])
+    scene.adjoint_records(P_d, s0, adj, (2.0 / n) * mean0.to(torch.float32), rec0, dc0, workspace=adj_ws)
     torch.cuda.synchronize()
     adj_work = _lib.work_counters(reset=True)
     wos.set_work_counting(False)
+    del rec0, dc0
 
     # -- warm-up
     for w in range(args.warmup):
@@ -334,18 +337,29 @@ def main():
     barrier()
     torch.cuda.synchronize()
     clocks.start()
-    times = []
+    step_times = []
     for k in range(args.steps):
         flush.zero_()
-        step(1000 * rank + k, times)
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        step(1000 * rank + k)
+        e1.record(stream)
+        step_times.append((e0, e1))
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
-    t_solve = [a.elapsed_time(b) * 1e-3 for a, b, _ in times]
-    t_adj = [b.elapsed_time(c) * 1e-3 for _, b, c in times]
-    t_step = float(np.sum(t_solve) + np.sum(t_adj))
+    t_step = float(sum(a.elapsed_time(b) for a, b in step_times)) * 1e-3
     t_max = max_over_ranks(t_step)
     status = wos.device_status(reset=False)
+
+    # -- per-kernel breakdown (separate, untimed for `value`)
+    times = []
+    for k in range(max(2, min(args.steps, 3))):
+        flush.zero_()
+        split_step(2000 + k, times)
+    torch.cuda.synchronize()
+    t_solve = [a.elapsed_time(b) * 1e-3 for a, b, _ in times]
+    t_adj = [b.elapsed_time(c) * 1e-3 for _, b, c in times]
 
     total_walks = world * n * NWALKS * args.steps
     value = total_walks / t_max
@@ -379,14 +393,15 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(n),
         "adjoint_pts_per_s": world * n * args.steps / t_max,
-        "breakdown_ms": {"forward": float(np.mean(t_solve)) * 1e3, "adjoint": adj_avg * 1e3},
+        "breakdown_ms": {"forward_kernel_and_reduce": float(np.mean(t_solve)) * 1e3, "adjoint": adj_avg * 1e3,
+                         "note": "separate calls of the fused step's kernels"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "kernel": "k_adjoint", "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": adj_bytes,
                      "work_per_launch": adj_work, "forward_work_per_launch": fwd_work,
                      "issue": {"achieved_tflops": adj_flops / adj_avg / 1e12, "peak_tflops": fp32_peak / 1e12,
                                "frac": adj_flops / adj_avg / fp32_peak}},
-        "gpu_launches": args.steps * 6,
+        "gpu_launches": args.steps * 7,
         "device_status": status,
         "plain_vs_persistent": plain,
     }

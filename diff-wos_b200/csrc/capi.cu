@@ -264,7 +264,7 @@ int wos_walk_records(wos_scene_t scene, const float *P, int n, const wos_params 
     cudaStream_t st = (cudaStream_t)stream;
     Scratch s;
     if (int rc = s.init(nullptr, 0, 256, st)) return rc;
-    WalkOut o{nullptr, nullptr, valid, pt, normal, t_or_uv, prim, contrib};
+    WalkOut o{nullptr, nullptr, nullptr, nullptr, valid, pt, normal, t_or_uv, prim, contrib};
     return launch_walk(scene->impl, P, n, *p, true, o, (unsigned long long *)s.base, st);
 }
 
@@ -280,7 +280,7 @@ int wos_walk_values(wos_scene_t scene, const float *P, int n, const wos_params *
     cudaStream_t st = (cudaStream_t)stream;
     Scratch s;
     if (int rc = s.init(nullptr, 0, 256, st)) return rc;
-    WalkOut o{values, steps, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    WalkOut o{values, steps, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     return launch_walk(scene->impl, P, (long long)n * p->nwalks, *p, false, o, (unsigned long long *)s.base, st);
 }
 
@@ -314,7 +314,7 @@ int wos_solve(wos_scene_t scene, const float *P, int n, const wos_params *p, dou
     if (int rc = s.init(workspace, workspace_bytes, wos_solve_workspace_size(n, p), st)) return rc;
     unsigned long long *counter = (unsigned long long *)s.base;
     float *vals = (float *)(s.base + 256);
-    WalkOut o{vals, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    WalkOut o{vals, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     if (int rc = launch_walk(scene->impl, P, (long long)n * p->nwalks, *p, false, o, counter, st)) return rc;
     return launch_reduce(vals, n, p->nwalks, mean, var, st);
 }
@@ -343,7 +343,7 @@ int wos_normal_derivative(wos_scene_t scene, const uint8_t *valid, const float *
     o.rtuv = t_or_uv;
     o.rprim = prim;
     o.nd = out;
-    return launch_adjoint(scene->impl, nullptr, n, *p, make_adj(*a), nullptr, true, o, (unsigned long long *)s.base,
+    return launch_adjoint(scene->impl, nullptr, n, *p, make_adj(*a), nullptr, ADJ_ND_ONLY, o, (unsigned long long *)s.base,
                           st);
 }
 
@@ -384,7 +384,7 @@ int wos_adjoint(wos_scene_t scene, const float *P, int n, const wos_params *p, c
     o.dV = aV;
     o.dg = ag;
     o.dsrc = as;
-    if (int rc = launch_adjoint(S, P, (long long)n * p->nwalks, *p, make_adj(*a), dLdu, false, o, counter, st))
+    if (int rc = launch_adjoint(S, P, (long long)n * p->nwalks, *p, make_adj(*a), dLdu, ADJ_RECOMPUTE, o, counter, st))
         return rc;
     if (a->want_dV)
         if (int rc = launch_add_f64(aV, dV, (long long)S.nV * S.dim, st)) return rc;
@@ -393,6 +393,172 @@ int wos_adjoint(wos_scene_t scene, const float *P, int n, const wos_params *p, c
     if (a->want_dsrc)
         if (int rc = launch_add_f64(as, dsrc, 5, st)) return rc;
     return 0;
+}
+
+size_t wos_walk_record_bytes(int dim) { return dim == 3 ? 16 : 8; }
+
+static bool wants_wds(const SceneImpl &S, const wos_params &p, const wos_adjoint_params &a) {
+    return a.want_dsrc && p.include_source && S.src_type != 0 && S.dim == 2;
+}
+
+// Adjoint accumulators (double) at the start of a workspace region.
+struct AdjAcc {
+    double *dV, *dg, *ds;
+    size_t bytes;
+};
+static AdjAcc adj_acc(const SceneImpl &S, char *base) {
+    AdjAcc r;
+    r.dV = (double *)base;
+    r.dg = (double *)((char *)r.dV + align256(sizeof(double) * (size_t)S.nV * S.dim));
+    r.ds = (double *)((char *)r.dg + align256(sizeof(double) * (size_t)S.nV));
+    r.bytes = align256(sizeof(double) * (size_t)S.nV * S.dim) + align256(sizeof(double) * (size_t)S.nV) + 256;
+    return r;
+}
+
+static int finish_adjoint(const SceneImpl &S, const wos_adjoint_params *a, const AdjAcc &acc, float *dV, float *dg,
+                          float *dsrc, cudaStream_t st) {
+    if (a->want_dV)
+        if (int rc = launch_add_f64(acc.dV, dV, (long long)S.nV * S.dim, st)) return rc;
+    if (a->want_dg)
+        if (int rc = launch_add_f64(acc.dg, dg, S.nV, st)) return rc;
+    if (a->want_dsrc)
+        if (int rc = launch_add_f64(acc.ds, dsrc, 5, st)) return rc;
+    return 0;
+}
+
+size_t wos_solve_adjoint_workspace_size(wos_scene_t scene, int n, const wos_params *p, const wos_adjoint_params *a) {
+    if (scene == nullptr || p == nullptr || a == nullptr || n < 0 || p->nwalks < 1) return 0;
+    const SceneImpl &S = scene->impl;
+    const size_t nw = (size_t)n * (size_t)p->nwalks;
+    size_t b = 256;                                                   // queue counter
+    b += align256(sizeof(float) * nw);                                // per-walk values
+    b += align256(wos_walk_record_bytes(S.dim) * nw);                 // per-walk records
+    if (wants_wds(S, *p, *a)) b += align256(sizeof(float) * 5 * nw);  // per-walk source derivatives
+    b += align256(sizeof(float) * (size_t)n);                         // dL/du
+    b += adj_acc(S, nullptr).bytes;                                   // gradient accumulators
+    return b;
+}
+
+int wos_solve_adjoint(wos_scene_t scene, const float *P, int n, const wos_params *p, const wos_adjoint_params *a,
+                      int loss_kind, const float *target_or_dLdu, double *mean, double *var, double *loss, float *dV,
+                      float *dg, float *dsrc, void *workspace, size_t workspace_bytes, wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (int rc = check_params(p)) return rc;
+    if (int rc = check_adj(a)) return rc;
+    if (n < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "n must be >= 0");
+    if (loss_kind < 0 || loss_kind > 2) return fail(WOS_ERR_INVALID_ARGUMENT, "loss_kind must be 0, 1 or 2");
+    if (loss_kind != 1 && target_or_dLdu == nullptr)
+        return fail(WOS_ERR_INVALID_ARGUMENT, "target_or_dLdu is NULL for this loss_kind");
+    if (n == 0) return 0;
+    if (a->want_dV && dV == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "want_dV set but dV is NULL");
+    if (a->want_dg && dg == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "want_dg set but dg is NULL");
+    if (a->want_dsrc && dsrc == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "want_dsrc set but dsrc is NULL");
+    WOS_CHECK_DEV(P, "P");
+    WOS_CHECK_DEV(mean, "mean");
+    WOS_CHECK_DEV_OPT(var, "var");
+    WOS_CHECK_DEV_OPT(loss, "loss");
+    WOS_CHECK_DEV_OPT(target_or_dLdu, "target_or_dLdu");
+    WOS_CHECK_DEV_OPT(dV, "dV");
+    WOS_CHECK_DEV_OPT(dg, "dg");
+    WOS_CHECK_DEV_OPT(dsrc, "dsrc");
+    const SceneImpl &S = scene->impl;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t need = wos_solve_adjoint_workspace_size(scene, n, p, a);
+    Scratch s;
+    if (int rc = s.init(workspace, workspace_bytes, need, st)) return rc;
+    const size_t nw = (size_t)n * (size_t)p->nwalks;
+    char *b = s.base;
+    unsigned long long *counter = (unsigned long long *)b;
+    b += 256;
+    float *vals = (float *)b;
+    b += align256(sizeof(float) * nw);
+    int *wrec = (int *)b;
+    b += align256(wos_walk_record_bytes(S.dim) * nw);
+    float *wds = nullptr;
+    if (wants_wds(S, *p, *a)) {
+        wds = (float *)b;
+        b += align256(sizeof(float) * 5 * nw);
+    }
+    float *dLdu = (float *)b;
+    b += align256(sizeof(float) * (size_t)n);
+    const AdjAcc acc = adj_acc(S, b);
+    cudaError_t e = cudaMemsetAsync(b, 0, acc.bytes, st);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(adjoint accumulators)");
+    WalkOut o{vals, nullptr, wrec, wds, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    if (int rc = launch_walk(S, P, (long long)nw, *p, false, o, counter, st)) return rc;
+    if (int rc = launch_reduce(vals, n, p->nwalks, mean, var, st)) return rc;
+    if (int rc = launch_loss(mean, n, loss_kind, target_or_dLdu, dLdu, loss, st)) return rc;
+    AdjOut ao{};
+    ao.dV = acc.dV;
+    ao.dg = acc.dg;
+    ao.dsrc = acc.ds;
+    ao.wrec = wrec;
+    ao.wds = wds;
+    if (int rc = launch_adjoint(S, P, (long long)nw, *p, make_adj(*a), dLdu, ADJ_FROM_RECORDS, ao, counter, st))
+        return rc;
+    return finish_adjoint(S, a, acc, dV, dg, dsrc, st);
+}
+
+int wos_solve_records(wos_scene_t scene, const float *P, int n, const wos_params *p, double *mean, double *var,
+                      void *records, float *dcontrib, void *workspace, size_t workspace_bytes, wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (int rc = check_params(p)) return rc;
+    if (n < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "n must be >= 0");
+    if (n == 0) return 0;
+    WOS_CHECK_DEV(P, "P");
+    WOS_CHECK_DEV(mean, "mean");
+    WOS_CHECK_DEV_OPT(var, "var");
+    WOS_CHECK_DEV(records, "records");
+    WOS_CHECK_DEV_OPT(dcontrib, "dcontrib");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch s;
+    if (int rc = s.init(workspace, workspace_bytes, wos_solve_workspace_size(n, p), st)) return rc;
+    unsigned long long *counter = (unsigned long long *)s.base;
+    float *vals = (float *)(s.base + 256);
+    WalkOut o{vals, nullptr, (int *)records, dcontrib, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    if (int rc = launch_walk(scene->impl, P, (long long)n * p->nwalks, *p, false, o, counter, st)) return rc;
+    return launch_reduce(vals, n, p->nwalks, mean, var, st);
+}
+
+int wos_adjoint_records(wos_scene_t scene, const float *P, int n, const wos_params *p, const wos_adjoint_params *a,
+                        const float *dLdu, const void *records, const float *dcontrib, float *dV, float *dg,
+                        float *dsrc, void *workspace, size_t workspace_bytes, wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (int rc = check_params(p)) return rc;
+    if (int rc = check_adj(a)) return rc;
+    if (n < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "n must be >= 0");
+    if (n == 0) return 0;
+    const SceneImpl &S = scene->impl;
+    if (a->want_dV && dV == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "want_dV set but dV is NULL");
+    if (a->want_dg && dg == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "want_dg set but dg is NULL");
+    if (a->want_dsrc && dsrc == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "want_dsrc set but dsrc is NULL");
+    if (wants_wds(S, *p, *a) && dcontrib == nullptr)
+        return fail(WOS_ERR_INVALID_ARGUMENT, "source gradient requested but dcontrib is NULL");
+    WOS_CHECK_DEV(P, "P");
+    WOS_CHECK_DEV(dLdu, "dLdu");
+    WOS_CHECK_DEV(records, "records");
+    WOS_CHECK_DEV_OPT(dcontrib, "dcontrib");
+    WOS_CHECK_DEV_OPT(dV, "dV");
+    WOS_CHECK_DEV_OPT(dg, "dg");
+    WOS_CHECK_DEV_OPT(dsrc, "dsrc");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t need = wos_adjoint_workspace_size(scene);
+    Scratch s;
+    if (int rc = s.init(workspace, workspace_bytes, need, st)) return rc;
+    unsigned long long *counter = (unsigned long long *)s.base;
+    const AdjAcc acc = adj_acc(S, s.base + 256);
+    cudaError_t e = cudaMemsetAsync(s.base, 0, need, st);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(adjoint workspace)");
+    AdjOut ao{};
+    ao.dV = acc.dV;
+    ao.dg = acc.dg;
+    ao.dsrc = acc.ds;
+    ao.wrec = (const int *)records;
+    ao.wds = dcontrib;
+    if (int rc = launch_adjoint(S, P, (long long)n * p->nwalks, *p, make_adj(*a), dLdu, ADJ_FROM_RECORDS, ao, counter,
+                                st))
+        return rc;
+    return finish_adjoint(S, a, acc, dV, dg, dsrc, st);
 }
 
 int wos_set_work_counting(int enable) { return set_work_counting(enable); }

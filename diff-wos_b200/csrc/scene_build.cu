@@ -360,6 +360,59 @@ __global__ void k_leaf_data(const unsigned long long *keys, int n, const float4 
     }
 }
 
+// Wide-tree boxes.  Level 1 node i bounds Morton positions [32 i, 32 i + 32).
+template <int D>
+__global__ void k_wt_level1(const unsigned long long *keys, int nF, const float *pbox, float4 *out, int n1) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n1) return;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    const int e = min(32 * i + 32, nF);
+    for (int s = 32 * i; s < e; ++s) {
+        const float *b = pbox + (size_t)(unsigned)keys[s] * 2 * D;
+        for (int k = 0; k < D; ++k) {
+            lo[k] = fminf(lo[k], b[k]);
+            hi[k] = fmaxf(hi[k], b[D + k]);
+        }
+    }
+    if (D == 2) {
+        out[i] = make_float4(lo[0], lo[1], hi[0], hi[1]);
+    } else {
+        out[2 * i] = make_float4(lo[0], lo[1], lo[2], 0.0f);
+        out[2 * i + 1] = make_float4(hi[0], hi[1], hi[2], 0.0f);
+    }
+}
+
+template <int D>
+__global__ void k_wt_level(const float4 *in, int n_in, float4 *out, int n_out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_out) return;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    const int e = min(32 * i + 32, n_in);
+    for (int c = 32 * i; c < e; ++c) {
+        if (D == 2) {
+            const float4 b = in[c];
+            lo[0] = fminf(lo[0], b.x);
+            lo[1] = fminf(lo[1], b.y);
+            hi[0] = fmaxf(hi[0], b.z);
+            hi[1] = fmaxf(hi[1], b.w);
+        } else {
+            const float4 a = in[2 * c], b = in[2 * c + 1];
+            lo[0] = fminf(lo[0], a.x);
+            lo[1] = fminf(lo[1], a.y);
+            lo[2] = fminf(lo[2], a.z);
+            hi[0] = fmaxf(hi[0], b.x);
+            hi[1] = fmaxf(hi[1], b.y);
+            hi[2] = fmaxf(hi[2], b.z);
+        }
+    }
+    if (D == 2) {
+        out[i] = make_float4(lo[0], lo[1], hi[0], hi[1]);
+    } else {
+        out[2 * i] = make_float4(lo[0], lo[1], lo[2], 0.0f);
+        out[2 * i + 1] = make_float4(hi[0], hi[1], hi[2], 0.0f);
+    }
+}
+
 // ------------------------------------------------------------------ host
 static inline int nblk(long long n, int b) { return (int)((n + b - 1) / b); }
 
@@ -370,7 +423,7 @@ static cudaError_t dalloc(T **p, size_t count, cudaStream_t st) {
 }
 
 void SceneImpl::release(cudaStream_t st) {
-    void *ptrs[] = {V, F, N, g, seg, seginv, tri, node, lseg, lseginv, ltri, lorig, cdf};
+    void *ptrs[] = {V, F, N, g, seg, seginv, tri, node, lseg, lseginv, ltri, lorig, cdf, wt_box, guide};
     for (void *p : ptrs)
         if (p) cudaFreeAsync(p, st);
     V = nullptr;
@@ -386,6 +439,8 @@ void SceneImpl::release(cudaStream_t st) {
     ltri = nullptr;
     lorig = nullptr;
     cdf = nullptr;
+    wt_box = nullptr;
+    guide = nullptr;
 }
 
 // Normalised CDF of pmf_i ~ r_i log(1/r_i), r_i = (i + 0.5)/n, built in
@@ -406,6 +461,17 @@ void build_g_cdf(std::vector<float> &cdf, int n) {
         cdf[i] = (float)(acc / total);
     }
     cdf[n - 1] = 1.0f;
+}
+
+void build_g_guide(const std::vector<float> &cdf, int ng, std::vector<unsigned short> &guide) {
+    const int n = (int)cdf.size();
+    guide.resize(ng + 1);
+    int l = 0;
+    for (int k = 0; k <= ng; ++k) {
+        const float u = (float)k / (float)ng;
+        while (l < n - 1 && !(u < cdf[l])) ++l;
+        guide[k] = (unsigned short)l;
+    }
 }
 
 template <int D>
@@ -487,6 +553,32 @@ static int build_geometry(SceneImpl &S, cudaStream_t st) {
     }
     k_leaf_data<D><<<nblk(nF, TB), TB, 0, st>>>(skeys, nF, S.seg, S.seginv, S.tri, S.lseg, S.lseginv, S.ltri, S.lorig);
 
+    // ---- wide tree (levels 1..wt_levels, the top one with <= 32 nodes)
+    {
+        const int W = D == 2 ? 1 : 2;  // float4 per box
+        int count = (nF + 31) / 32, level = 1, off = 0;
+        S.wt_count[0] = nF;
+        for (;;) {
+            if (level > WT_MAX_LEVELS) return fail(WOS_ERR_UNSUPPORTED, "scene too large for the wide tree");
+            S.wt_count[level] = count;
+            S.wt_off[level] = off;
+            off += count;
+            if (count <= 32) break;
+            count = (count + 31) / 32;
+            ++level;
+        }
+        S.wt_levels = level;
+        if (S.wt_box) cudaFreeAsync(S.wt_box, st);
+        S.wt_box = nullptr;
+        WOS_TRY(dalloc(&S.wt_box, (size_t)off * W, st));
+        k_wt_level1<D><<<nblk(S.wt_count[1], TB), TB, 0, st>>>(skeys, nF, pbox, S.wt_box, S.wt_count[1]);
+        for (int l = 2; l <= S.wt_levels; ++l)
+            k_wt_level<D><<<nblk(S.wt_count[l], TB), TB, 0, st>>>(S.wt_box + (size_t)S.wt_off[l - 1] * W,
+                                                                S.wt_count[l - 1], S.wt_box + (size_t)S.wt_off[l] * W,
+                                                                S.wt_count[l]);
+        WOS_TRY(cudaGetLastError());
+    }
+
     // ---- hierarchy
     const int nInt = nF - 1;
     S.nNodes = nInt;
@@ -564,8 +656,13 @@ int SceneImpl::allocate(cudaStream_t st) {
     std::vector<float> c;
     build_g_cdf(c, 10000);
     n_cdf = (int)c.size();
+    std::vector<unsigned short> gd;
+    n_guide = 2048;
+    build_g_guide(c, n_guide, gd);
     WOS_TRY(dalloc(&cdf, c.size(), st));
+    WOS_TRY(dalloc(&guide, gd.size(), st));
     WOS_TRY(cudaMemcpyAsync(cdf, c.data(), c.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    WOS_TRY(cudaMemcpyAsync(guide, gd.data(), gd.size() * sizeof(unsigned short), cudaMemcpyHostToDevice, st));
     WOS_TRY(cudaStreamSynchronize(st));
     return 0;
 }
@@ -613,6 +710,14 @@ SceneView SceneImpl::view() const {
     for (int k = 0; k < 5; ++k) v.src[k] = src[k];
     v.cdf = cdf;
     v.n_cdf = n_cdf;
+    v.guide = guide;
+    v.n_guide = n_guide;
+    v.wt_levels = wt_levels;
+    for (int k = 0; k < 8; ++k) {
+        v.wt_count[k] = wt_count[k];
+        v.wt_off[k] = wt_off[k];
+    }
+    v.wt_box = wt_box;
     return v;
 }
 

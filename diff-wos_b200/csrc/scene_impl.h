@@ -17,6 +17,7 @@ int fail(int code, const std::string &msg);
 int fail_cuda(cudaError_t e, const char *where);
 
 void build_g_cdf(std::vector<float> &cdf, int n);
+void build_g_guide(const std::vector<float> &cdf, int ng, std::vector<unsigned short> &guide);
 
 // Owns every device buffer of one scene.  Geometry buffers are immutable
 // between wos_scene_update_* calls.
@@ -43,6 +44,12 @@ struct SceneImpl {
     float src[5] = {0, 0, 0, 0, 0};
     float *cdf = nullptr;
     int n_cdf = 0;
+    unsigned short *guide = nullptr;
+    int n_guide = 0;
+    int wt_levels = 0;
+    int wt_count[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int wt_off[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    float4 *wt_box = nullptr;
 
     int allocate(cudaStream_t st);
     int check_indices(cudaStream_t st);

@@ -58,14 +58,51 @@ __device__ __forceinline__ Hit query(const SceneView &S, const float *p, const f
 }
 
 // Add a warp's work counters to the global totals (counting launches only).
+// Cooperative queries count once per warp (every lane holds the same totals).
+template <bool COOP>
 __device__ __forceinline__ void flush_work(const Work &wk) {
     unsigned long long v[3] = {wk.nq, wk.nb, wk.np};
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
+        if (!COOP) {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+        }
         if ((threadIdx.x & 31) == 0) atomicAdd(&g_work[k], v[k]);
     }
+}
+
+// Nearest query of every active lane.  With the LBVH the lanes take turns:
+// the whole warp answers each lane's query cooperatively (wquery), starting
+// from the warm candidate `warm` (that lane's previous nearest primitive, or
+// -1).  Brute force runs per lane.  Must be called by all 32 lanes.
+template <int D, bool BVH>
+__device__ __forceinline__ Hit warp_queries(const SceneView &S, bool active, const float *x, int warm, Work &work) {
+    Hit mine{-1, INFINITY};
+    if (!BVH) {
+        if (active) mine = nearest_brute<D>(S, x, work);
+        return mine;
+    }
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    unsigned act = __ballot_sync(FULL, active);
+    while (act) {
+        const int j = __ffs(act) - 1;
+        act &= act - 1u;
+        float q[3];
+        q[0] = __shfl_sync(FULL, x[0], j);
+        q[1] = __shfl_sync(FULL, x[1], j);
+        q[2] = D == 3 ? __shfl_sync(FULL, x[2], j) : 0.0f;
+        const int wp = __shfl_sync(FULL, warm, j);
+        Hit best{-1, INFINITY};
+        if (wp >= 0) {
+            best.prim = wp;
+            best.d2 = prim_d2<D>(S, wp, q);
+        }
+        const Hit h = wquery<D>(S, q, best, work);
+        if (lane == j) mine = h;
+    }
+    return mine;
 }
 
 // ------------------------------------------------------------------ walker
@@ -76,6 +113,7 @@ struct Walker {
     float contrib;
     float ds[5];
     int i;
+    int last;  // nearest primitive of the previous query (warm start), -1 if none
     bool fresh;
     __device__ __forceinline__ void start(const float *x, int D) {
         p[0] = x[0];
@@ -85,6 +123,7 @@ struct Walker {
 #pragma unroll
         for (int k = 0; k < 5; ++k) ds[k] = 0.0f;
         i = 0;
+        last = -1;
         fresh = true;
     }
 };
@@ -94,7 +133,7 @@ struct Walker {
 template <int D>
 __device__ __forceinline__ int walker_advance(Walker &w, const SceneView &S, const Hit &hit, const WalkCfg &c,
                                               float eps, bool project, bool prevent_fd, uint32_t pt, uint32_t wk,
-                                              uint32_t role, bool want_ds, const float *cdf) {
+                                              uint32_t role, bool want_ds, const unsigned short *guide) {
     float d = sqrtf(hit.d2);
     if (w.fresh) {
         w.fresh = false;
@@ -107,7 +146,7 @@ __device__ __forceinline__ int walker_advance(Walker &w, const SceneView &S, con
         const uint4 r = philox(c.rng, pt, wk, (uint32_t)w.i, role);
         if (D == 2 && S.src_type != 0) {
             float yx, yy;
-            const float K = source_step(S, cdf, c.use_IS != 0, w.p[0], w.p[1], d, r.z, r.w, yx, yy);
+            const float K = source_step(S, guide, c.use_IS != 0, w.p[0], w.p[1], d, r.z, r.w, yx, yy);
             float df[5];
             const float f = source(S, yx, yy, want_ds ? df : nullptr);
             w.contrib = fmaf(f, K, w.contrib);
@@ -136,21 +175,33 @@ __device__ __forceinline__ int walker_advance(Walker &w, const SceneView &S, con
     return project ? W_VALID : W_TRUNC;
 }
 
-// Stage the shallowest LBVH nodes and (optionally) the G CDF in shared memory.
-template <int D, bool BVH>
-__device__ __forceinline__ void stage_smem(const SceneView &S, int n_top, bool stage_cdf, float4 *smem,
-                                           const float4 *&top, const float *&cdf) {
-    constexpr int K = NodeWords<D>::K;
-    const int nt = BVH ? n_top : 0;
-    for (int t = threadIdx.x; t < nt * K; t += blockDim.x) smem[t] = S.node[t];
-    float *scdf = reinterpret_cast<float *>(smem + nt * K);
-    cdf = S.cdf;
-    if (stage_cdf) {
-        for (int t = threadIdx.x; t < S.n_cdf; t += blockDim.x) scdf[t] = S.cdf[t];
-        cdf = scdf;
+// Dynamic shared memory: [G-CDF guide table][per-thread scratch of
+// `thread_words` 8-byte words].
+__host__ __device__ inline size_t smem_bytes(int n_guide, int nthreads, int thread_words) {
+    size_t b = ((size_t)(n_guide + 1) * sizeof(unsigned short) + 15) & ~(size_t)15;
+    b += (size_t)nthreads * thread_words * 8;
+    return b;
+}
+
+struct Smem {
+    const unsigned short *guide;
+    double *scratch;  // this thread's words
+};
+
+__device__ __forceinline__ Smem stage_smem(const SceneView &S, bool stage_guide, int thread_words, float4 *smem) {
+    Smem m;
+    char *base = reinterpret_cast<char *>(smem);
+    const int ng = stage_guide ? S.n_guide : -1;
+    unsigned short *sg = reinterpret_cast<unsigned short *>(base);
+    m.guide = S.guide;
+    if (stage_guide) {
+        for (int t = threadIdx.x; t <= S.n_guide; t += blockDim.x) sg[t] = S.guide[t];
+        m.guide = sg;
     }
-    top = smem;
+    base += ((size_t)(ng + 1) * sizeof(unsigned short) + 15) & ~(size_t)15;
+    m.scratch = reinterpret_cast<double *>(base) + (size_t)threadIdx.x * thread_words;
     __syncthreads();
+    return m;
 }
 
 // Warp-uniform refill of idle lanes from chunks of the global index space.
@@ -199,14 +250,13 @@ __global__ void __launch_bounds__(512) k_walk(SceneView S, WalkCfg c, const floa
                                              unsigned long long *counter, int chunk, int n_top, int stage_cdf,
                                              WalkOut out) {
     extern __shared__ float4 smem[];
-    const float4 *top;
-    const float *cdf;
-    stage_smem<D, BVH>(S, n_top, stage_cdf != 0, smem, top, cdf);
+    const Smem sm = stage_smem(S, stage_cdf != 0, 0, smem);
     Queue q{0, 0, false};
     bool active = false;
     long long idx = 0;
     uint32_t pt = 0, wk = 0;
     Walker w;
+    w.last = -1;
     Work work{0, 0, 0};
     for (;;) {
         const bool was = active;
@@ -221,10 +271,11 @@ __global__ void __launch_bounds__(512) k_walk(SceneView S, WalkCfg c, const floa
             }
             w.start(P + (size_t)pt * D, D);
         }
+        const Hit hit = warp_queries<D, BVH>(S, active, w.p, w.last, work);
         if (!active) continue;
-        const Hit hit = query<D, BVH>(S, w.p, top, n_top, work);
+        w.last = hit.prim;
         const int r = walker_advance<D>(w, S, hit, c, c.eps, c.project != 0, c.prevent_fd != 0, pt, wk, ROLE_PRIMAL,
-                                        false, cdf);
+                                        out.wds != nullptr, sm.guide);
         if (r == W_CONTINUE) continue;
         active = false;
         if (RECORDS) {
@@ -245,17 +296,35 @@ __global__ void __launch_bounds__(512) k_walk(SceneView S, WalkCfg c, const floa
             if (out.contrib) out.contrib[pt] = ok ? w.contrib : 0.0f;
         } else {
             float v = 0.0f;
+            Rec rec;
             if (r == W_VALID) {
-                const Rec rec = closest_record<D>(S, w.p, hit.prim);
+                rec = closest_record<D>(S, w.p, hit.prim);
                 v = dirichlet<D>(S, hit.prim, rec.t0, rec.t1, nullptr, nullptr);
                 if (c.include_source) v += w.contrib;
                 if (!isfinite(v)) atomicOr(&g_status, ST_NONFINITE);
             }
             out.values[idx] = v;
+            if (out.wrec) {
+                if (D == 2) {
+                    const int2 wr = r == W_VALID ? make_int2(hit.prim | (rec.flip ? 0x40000000 : 0),
+                                                             __float_as_int(rec.t0))
+                                                 : make_int2(-1, 0);
+                    reinterpret_cast<int2 *>(out.wrec)[idx] = wr;
+                } else {
+                    const int4 wr = r == W_VALID ? make_int4(hit.prim | (rec.flip ? 0x40000000 : 0),
+                                                             __float_as_int(rec.t0), __float_as_int(rec.t1), 0)
+                                                 : make_int4(-1, 0, 0, 0);
+                    reinterpret_cast<int4 *>(out.wrec)[idx] = wr;
+                }
+            }
+            if (out.wds) {
+#pragma unroll
+                for (int k = 0; k < 5; ++k) out.wds[(size_t)idx * 5 + k] = r == W_VALID ? w.ds[k] : 0.0f;
+            }
             if (out.steps) out.steps[idx] = r == W_TRUNC ? c.nsteps : w.i;
         }
     }
-    if (c.count) flush_work(work);
+    if (c.count) flush_work<BVH>(work);
 }
 
 // Reference-shaped kernel: one thread per (point, walk), no regeneration.
@@ -273,7 +342,7 @@ __global__ void __launch_bounds__(256) k_walk_plain(SceneView S, WalkCfg c, cons
     for (;;) {
         const Hit hit = query<D, BVH>(S, w.p, nullptr, 0, work);
         const int r = walker_advance<D>(w, S, hit, c, c.eps, c.project != 0, c.prevent_fd != 0, pt, wk, ROLE_PRIMAL,
-                                        false, S.cdf);
+                                        false, S.guide);
         if (r == W_CONTINUE) continue;
         if (r == W_VALID) {
             const Rec rec = closest_record<D>(S, w.p, hit.prim);
@@ -533,20 +602,47 @@ __device__ __forceinline__ void nd_finish(const NdState &st, const SceneView &S,
 
 enum { PH_IDLE = 0, PH_PRIMAL = 1, PH_BALL = 2, PH_ANTI_START = 3, PH_ANTI_WALK = 4, PH_ND_START = 5 };
 
+// Per-thread adjoint state kept in shared memory: touched at phase changes,
+// not in the query loop, so it does not occupy registers.
+struct AdjSlot {
+    NdState st;
+    float rn[3];  // record normal (towards the interior)
+    float rt0, rt1;
+    float ba, bb;  // bisection bracket
+    int bk;
+    double acc[5];  // source-parameter gradient accumulators
+};
+constexpr int ADJ_THREAD_WORDS = (int)((sizeof(AdjSlot) + 7) / 8);
+
+// The adjoint kernel runs at most 256 threads per block and is compiled for
+// at least ADJ_MIN_BLOCKS resident blocks per SM (a register cap).
+#ifndef ADJ_MIN_BLOCKS
+#define ADJ_MIN_BLOCKS 3
+#endif
+
 // Persistent adjoint kernel.  ND_ONLY: the items are boundary records and the
 // kernel writes one normal-derivative estimate per record (the
 // wos_normal_derivative entry point); otherwise items are (point, walk)
 // samples and gradients are accumulated into dV / dg / dsrc.
-template <int D, bool BVH, bool ND_ONLY>
-__global__ void __launch_bounds__(512) k_adjoint(SceneView S, WalkCfg c, AdjCfg a, const float *__restrict__ P,
+template <int D, bool BVH, int MODE>
+__global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, WalkCfg c, AdjCfg a, const float *__restrict__ P,
                                                 long long total, const float *__restrict__ dLdu,
                                                 unsigned long long *counter, int chunk, int n_top, int stage_cdf,
                                                 AdjOut out) {
     extern __shared__ float4 smem[];
-    const float4 *top;
-    const float *cdf;
-    stage_smem<D, BVH>(S, n_top, stage_cdf != 0, smem, top, cdf);
+    const Smem sm = stage_smem(S, stage_cdf != 0, ADJ_THREAD_WORDS, smem);
+    const unsigned short *cdf = sm.guide;
+    AdjSlot &slot = *reinterpret_cast<AdjSlot *>(sm.scratch);
+    double *acc_src = slot.acc;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) acc_src[k] = 0.0;
+    NdState &st = slot.st;
+    float *rn = slot.rn;
+    float &rt0 = slot.rt0, &rt1 = slot.rt1;
+    float &ba = slot.ba, &bb = slot.bb;
+    int &bk = slot.bk;
     const bool src2 = D == 2 && S.src_type != 0;
+    constexpr bool ND_ONLY = MODE == ADJ_ND_ONLY;
     const bool want_src = !ND_ONLY && a.want_dsrc && c.include_source && src2;
     const bool with_src = a.source_in_nd && src2;
     Queue q{0, 0, false};
@@ -556,16 +652,13 @@ __global__ void __launch_bounds__(512) k_adjoint(SceneView S, WalkCfg c, AdjCfg 
     int phase = PH_IDLE;
     double W = 0.0;
     Walker w;
-    NdState st;
     int rprim = 0;
-    float rt0 = 0.0f, rt1 = 0.0f;
-    float rn[3] = {0, 0, 0};
     float qpos[3] = {0, 0, 0};
-    float ba = 0.0f, bb = 0.0f;
-    int bk = 0;
-    double acc_src[5] = {0, 0, 0, 0, 0};
     Work work{0, 0, 0};
+    w.last = -1;
 
+    // Every lane reaches warp_queries once per iteration: no `continue`
+    // between refill() and the query.
     for (;;) {
         const bool was = active;
         if (!refill(q, active, idx, counter, total, chunk)) break;
@@ -573,13 +666,14 @@ __global__ void __launch_bounds__(512) k_adjoint(SceneView S, WalkCfg c, AdjCfg 
             if (ND_ONLY) {
                 pt = (uint32_t)idx;
                 wk = c.walk_offset;
-                if (!out.rvalid[pt]) {
+                const int rp = out.rprim[pt];
+                if (!out.rvalid[pt] || rp < 0 || rp >= S.nF) {
+                    if (out.rvalid[pt]) atomicOr(&g_status, ST_BAD_PRIM);
 #pragma unroll
                     for (int k = 0; k < D; ++k) out.nd[(size_t)pt * D + k] = 0.0f;
                     active = false;
-                    continue;
                 }
-                rprim = out.rprim[pt];
+                rprim = active ? rp : 0;
                 rt0 = out.rtuv[2 * (size_t)pt];
                 rt1 = out.rtuv[2 * (size_t)pt + 1];
 #pragma unroll
@@ -592,16 +686,61 @@ __global__ void __launch_bounds__(512) k_adjoint(SceneView S, WalkCfg c, AdjCfg 
                 pt = (uint32_t)(idx / c.nwalks);
                 wk = c.walk_offset + (uint32_t)(idx - (long long)pt * c.nwalks);
                 W = (double)__ldg(&dLdu[pt]) / c.nwalks;
-                if (W == 0.0) {
-                    active = false;
-                    continue;
-                }
                 w.start(P + (size_t)pt * D, D);
                 phase = PH_PRIMAL;
+                if (W == 0.0) active = false;
+                if (MODE == ADJ_FROM_RECORDS && active) {
+                    // the primal walk ran in the forward pass: start from its record
+                    int code;
+                    if (D == 2) {
+                        const int2 wr = __ldg(reinterpret_cast<const int2 *>(out.wrec) + idx);
+                        code = wr.x;
+                        rt0 = __int_as_float(wr.y);
+                        rt1 = 0.0f;
+                    } else {
+                        const int4 wr = __ldg(reinterpret_cast<const int4 *>(out.wrec) + idx);
+                        code = wr.x;
+                        rt0 = __int_as_float(wr.y);
+                        rt1 = __int_as_float(wr.z);
+                    }
+                    if (code < 0) {
+                        active = false;
+                    } else {
+                        rprim = code & 0x3fffffff;
+                        const Rec rec = record_from<D>(S, rprim, rt0, rt1, (code & 0x40000000) != 0);
+                        int vid[3];
+                        float wts[3];
+                        st.uref = dirichlet<D>(S, rprim, rt0, rt1, vid, wts);
+                        if (a.want_dg) {
+#pragma unroll
+                            for (int s2 = 0; s2 < D; ++s2) atomicAdd(&out.dg[vid[s2]], W * (double)wts[s2]);
+                        }
+                        if (want_src) {
+#pragma unroll
+                            for (int k = 0; k < 5; ++k)
+                                acc_src[k] += W * (double)__ldg(&out.wds[(size_t)idx * 5 + k]);
+                        }
+                        if (!a.want_dV) {
+                            active = false;
+                        } else {
+#pragma unroll
+                            for (int k = 0; k < D; ++k) {
+                                st.p[k] = rec.p[k];
+                                rn[k] = rec.n[k];
+                            }
+                            ba = a.ball_eps;
+                            bb = S.half_min_extent;
+                            bk = 0;
+                            const float m = (ba + bb) * 0.5f;
+#pragma unroll
+                            for (int k = 0; k < D; ++k) qpos[k] = fmaf(rn[k], m, st.p[k]);
+                            phase = PH_BALL;
+                        }
+                    }
+                }
             }
         }
-        if (!active) continue;
-        if (phase == PH_ND_START) {
+        if (active && phase == PH_ND_START) {
             // no query needed to start: set up the bisection
             st.uref = dirichlet<D>(S, rprim, rt0, rt1, nullptr, nullptr);
             ba = a.ball_eps;
@@ -612,8 +751,13 @@ __global__ void __launch_bounds__(512) k_adjoint(SceneView S, WalkCfg c, AdjCfg 
             for (int k = 0; k < D; ++k) qpos[k] = fmaf(rn[k], m, st.p[k]);
             phase = PH_BALL;
         }
-        const float *x = (phase == PH_PRIMAL || phase == PH_ANTI_WALK) ? w.p : qpos;
-        const Hit hit = query<D, BVH>(S, x, top, n_top, work);
+        const bool walking = phase == PH_PRIMAL || phase == PH_ANTI_WALK;
+        float x[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) x[k] = walking ? w.p[k] : qpos[k];
+        const Hit hit = warp_queries<D, BVH>(S, active, x, walking ? w.last : rprim, work);
+        if (!active) continue;
+        if (walking) w.last = hit.prim;
         bool finish_anti = false;
         float uq = 0.0f;
         if (phase == PH_PRIMAL) {
@@ -689,6 +833,7 @@ __global__ void __launch_bounds__(512) k_adjoint(SceneView S, WalkCfg c, AdjCfg 
                 finish_anti = true;
             } else {
                 w.start(qpos, D);
+                w.last = hit.prim;
                 const int r = walker_advance<D>(w, S, hit, c, a.epsilon2, false, false, pt, wk, role, false, cdf);
                 if (r == W_CONTINUE) {
                     phase = PH_ANTI_WALK;
@@ -740,7 +885,7 @@ __global__ void __launch_bounds__(512) k_adjoint(SceneView S, WalkCfg c, AdjCfg 
             phase = PH_IDLE;
         }
     }
-    if (c.count) flush_work(work);
+    if (c.count) flush_work<BVH>(work);
     if (want_src) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
@@ -750,6 +895,40 @@ __global__ void __launch_bounds__(512) k_adjoint(SceneView S, WalkCfg c, AdjCfg 
             if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&out.dsrc[k], v);
         }
     }
+}
+
+// dL/du per point for a pointwise loss of the per-point means, and the loss
+// (one block, fixed reduction order).  kind 1: mean(u^2); kind 2:
+// mean((u - target)^2); kind 0: dL/du given.
+__global__ void k_loss(const double *mean, int n, int kind, const float *tg, float *dLdu, double *loss) {
+    __shared__ double red[1024];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double u = mean[i];
+        double e = u;
+        if (kind == 2) e = u - (double)tg[i];
+        if (kind == 0) {
+            dLdu[i] = tg[i];
+        } else {
+            dLdu[i] = (float)(2.0 * e / n);
+            acc += e * e / n;
+        }
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && loss) *loss = red[0];
+}
+
+int launch_loss(const double *mean, int n, int kind, const float *target_or_dLdu, float *dLdu, double *loss,
+                cudaStream_t st) {
+    k_loss<<<1, 1024, 0, st>>>(mean, n, kind, target_or_dLdu, dLdu, loss);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_loss launch");
+    return 0;
 }
 
 __global__ void k_add_f64_to_f32(const double *src, float *dst, long long n) {
@@ -812,13 +991,16 @@ struct Shape {
 };
 
 template <typename Kern>
-static int shape_for(Kern kern, const SceneImpl &S, int D, bool bvh, bool want_cdf, Shape &sh) {
+static int shape_for(Kern kern, const SceneImpl &S, int D, bool bvh, bool want_cdf, Shape &sh,
+                     int thread_words = 0, int max_block = 512) {
     const wos_launch_config &cfg = g_cfg[D - 2];
-    const int K = D == 2 ? 3 : 4;
-    sh.block = cfg.block_threads;
-    sh.n_top = bvh ? std::min(cfg.smem_nodes, S.nNodes) : 0;
+    sh.block = std::min(cfg.block_threads, max_block);
+    // the persistent kernels query the wide tree cooperatively; no binary-LBVH
+    // nodes are staged
+    sh.n_top = 0;
     sh.stage_cdf = want_cdf ? 1 : 0;
-    sh.smem = (size_t)sh.n_top * K * sizeof(float4) + (want_cdf ? (size_t)S.n_cdf * sizeof(float) : 0);
+    sh.smem = smem_bytes(want_cdf ? S.n_guide : -1, sh.block, thread_words);
+    (void)bvh;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -946,7 +1128,7 @@ int launch_ball(const SceneImpl &S, const uint8_t *valid, const float *pt, const
     return 0;
 }
 
-template <int D, bool BVH, bool ND>
+template <int D, bool BVH, int ND>
 static int launch_adjoint_t(const SceneImpl &S, const float *P, long long total, const wos_params &p,
                             const AdjCfg &a, const float *dLdu, const AdjOut &out, unsigned long long *counter,
                             cudaStream_t st) {
@@ -954,7 +1136,7 @@ static int launch_adjoint_t(const SceneImpl &S, const float *P, long long total,
     const WalkCfg c = make_cfg(p);
     const bool want_cdf = D == 2 && S.src_type != 0 && p.use_IS_for_greens;
     Shape sh;
-    int rc = shape_for(k_adjoint<D, BVH, ND>, S, D, BVH, want_cdf, sh);
+    int rc = shape_for(k_adjoint<D, BVH, ND>, S, D, BVH, want_cdf, sh, ADJ_THREAD_WORDS, 256);
     if (rc) return rc;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
@@ -967,12 +1149,15 @@ static int launch_adjoint_t(const SceneImpl &S, const float *P, long long total,
 }
 
 int launch_adjoint(const SceneImpl &S, const float *P, long long total, const wos_params &p, const AdjCfg &a,
-                   const float *dLdu, bool nd_only, const AdjOut &out, unsigned long long *counter, cudaStream_t st) {
+                   const float *dLdu, int mode, const AdjOut &out, unsigned long long *counter, cudaStream_t st) {
     if (total == 0) return 0;
     const bool bvh = p.use_bvh != 0;
-#define WOS_ADJ(D_, B_)                                                                               \
-    return nd_only ? launch_adjoint_t<D_, B_, true>(S, P, total, p, a, dLdu, out, counter, st)       \
-                   : launch_adjoint_t<D_, B_, false>(S, P, total, p, a, dLdu, out, counter, st)
+#define WOS_ADJ(D_, B_)                                                                                       \
+    return mode == ADJ_ND_ONLY                                                                                \
+               ? launch_adjoint_t<D_, B_, ADJ_ND_ONLY>(S, P, total, p, a, dLdu, out, counter, st)            \
+               : (mode == ADJ_FROM_RECORDS                                                                    \
+                      ? launch_adjoint_t<D_, B_, ADJ_FROM_RECORDS>(S, P, total, p, a, dLdu, out, counter, st) \
+                      : launch_adjoint_t<D_, B_, ADJ_RECOMPUTE>(S, P, total, p, a, dLdu, out, counter, st))
     if (S.dim == 2) {
         if (bvh) WOS_ADJ(2, true);
         WOS_ADJ(2, false);

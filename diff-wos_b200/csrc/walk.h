@@ -30,6 +30,8 @@ struct AdjCfg {
 struct WalkOut {
     float *values;
     int *steps;
+    int *wrec;   // per-walk WalkRec (walkrec_words(D) ints each), may be null
+    float *wds;  // per-walk source-parameter derivative (5 floats each), may be null
     uint8_t *valid;
     float *pt, *nrm, *tuv;
     int *prim;
@@ -49,7 +51,12 @@ struct AdjOut {
     const float *rpt, *rnrm, *rtuv;
     const int *rprim;
     float *nd;
+    // records mode: per-walk WalkRec and source derivatives from the forward pass
+    const int *wrec;
+    const float *wds;
 };
+
+enum AdjMode { ADJ_RECOMPUTE = 0, ADJ_ND_ONLY = 1, ADJ_FROM_RECORDS = 2 };
 
 WalkCfg make_cfg(const wos_params &p);
 int read_status(int reset, int *out);
@@ -67,7 +74,9 @@ int launch_closest(const SceneImpl &S, const float *P, int n, bool bvh, const Qu
 int launch_ball(const SceneImpl &S, const uint8_t *valid, const float *pt, const float *nrm, int n, float eps,
                 bool bvh, float *R, cudaStream_t st);
 int launch_adjoint(const SceneImpl &S, const float *P, long long total, const wos_params &p, const AdjCfg &a,
-                   const float *dLdu, bool nd_only, const AdjOut &out, unsigned long long *counter, cudaStream_t st);
+                   const float *dLdu, int mode, const AdjOut &out, unsigned long long *counter, cudaStream_t st);
+int launch_loss(const double *mean, int n, int kind, const float *target_or_dLdu, float *dLdu, double *loss,
+                cudaStream_t st);
 int launch_add_f64(const double *src, float *dst, long long n, cudaStream_t st);
 
 }  // namespace wosd

@@ -56,7 +56,23 @@ struct SceneView {
     float src[5];
     const float *cdf;  // G CDF table (n_cdf entries)
     int n_cdf;
+    // guide[k] = first index l with cdf[l] > k / n_guide (k = 0..n_guide):
+    // brackets the CDF search to a few entries
+    const unsigned short *guide;
+    int n_guide;
+    // Wide tree for the warp-cooperative query: an implicit 32-ary tree over
+    // the Morton-ordered primitives.  Level 1 node i bounds primitives
+    // [32 i, 32 i + 32) (in Morton order), level k node i bounds level k-1
+    // nodes [32 i, 32 i + 32); level wt_levels has at most 32 nodes.  Boxes:
+    // 2D one float4 (lo.x, lo.y, hi.x, hi.y) per node, 3D two float4
+    // (lo.xyz, 0), (hi.xyz, 0); level k starts at wt_box[wt_off[k]] (in nodes).
+    int wt_levels;
+    int wt_count[8];
+    int wt_off[8];
+    const float4 *wt_box;
 };
+
+constexpr int WT_MAX_LEVELS = 5;
 
 template <int D>
 struct NodeWords;
@@ -380,13 +396,130 @@ __device__ __forceinline__ Hit nearest_bvh(const SceneView &S, const float *p, c
     return h;
 }
 
+// ------------------------------------------------------------------ wide tree
+// Warp minimum of a non-negative float (or +inf): for such values the IEEE
+// bit pattern orders like the value, so one redux.sync integer minimum does it.
+__device__ __forceinline__ float warp_min(float v) {
+    return __uint_as_float(__reduce_min_sync(0xffffffffu, __float_as_uint(v)));
+}
+__device__ __forceinline__ int warp_min_int(int v) { return __reduce_min_sync(0xffffffffu, v); }
+
+template <int D>
+__device__ __forceinline__ float wt_box_d2(const SceneView &S, int node, const float *q) {
+    float lo[3], hi[3];
+    if (D == 2) {
+        const float4 b = __ldg(&S.wt_box[node]);
+        lo[0] = b.x;
+        lo[1] = b.y;
+        hi[0] = b.z;
+        hi[1] = b.w;
+    } else {
+        const float4 a = __ldg(&S.wt_box[2 * node]), b = __ldg(&S.wt_box[2 * node + 1]);
+        lo[0] = a.x;
+        lo[1] = a.y;
+        lo[2] = a.z;
+        hi[0] = b.x;
+        hi[1] = b.y;
+        hi[2] = b.z;
+    }
+    return box_d2<D>(lo, hi, q);
+}
+
+// Squared distance to the primitive at Morton position s.
+template <int D>
+__device__ __forceinline__ float leaf_d2(const SceneView &S, int s, const float *q) {
+    if (D == 2) {
+        float t;
+        return seg_d2(__ldg(&S.lseg[s]), __ldg(&S.lseginv[s]), q[0], q[1], t);
+    }
+    return tri_d2(__ldg(&S.ltri[3 * s]), __ldg(&S.ltri[3 * s + 1]), __ldg(&S.ltri[3 * s + 2]), q[0], q[1], q[2]);
+}
+
+// Squared distance to primitive f in the original order.
+template <int D>
+__device__ __forceinline__ float prim_d2(const SceneView &S, int f, const float *q) {
+    if (D == 2) {
+        float t;
+        return seg_d2(__ldg(&S.seg[f]), __ldg(&S.seginv[f]), q[0], q[1], t);
+    }
+    return tri_d2(__ldg(&S.tri[3 * f]), __ldg(&S.tri[3 * f + 1]), __ldg(&S.tri[3 * f + 2]), q[0], q[1], q[2]);
+}
+
+// Warp-cooperative nearest primitive for one query point q (the same q in
+// every lane; every lane returns the same Hit).  Best-first descent of the
+// wide tree, one template instance per level: the level's frontier of up to
+// 32 child distances is one register per lane, the nearest unexpanded child
+// is a redux.sync minimum, and a node expansion is one coalesced load of 32
+// boxes or 32 primitives.  `best` may hold a warm-start candidate (a real
+// primitive with its distance); pruning is conservative, so the result is the
+// exact minimum of (d2, primitive index) -- the same as the brute-force search.
+template <int D, int L>
+__device__ __forceinline__ void wdescend(const SceneView &S, const float *q, int first, float tol2, Hit &best,
+                                         Work &wk) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int child = first + lane;
+    float d = INFINITY;
+    if (child < S.wt_count[L]) d = wt_box_d2<D>(S, S.wt_off[L] + child, q);
+    wk.nb += 1;
+    for (;;) {
+        const float m = warp_min(d);
+        if (m > prune_bound(best.d2, tol2)) return;
+        const int j = __ffs(__ballot_sync(FULL, d == m)) - 1;
+        if (lane == j) d = INFINITY;
+        const int node = first + j;
+        if constexpr (L == 1) {
+            wk.np += 1;
+            const int s = node * 32 + lane;
+            float d2 = INFINITY;
+            if (s < S.nF) d2 = leaf_d2<D>(S, s, q);
+            const float m2 = warp_min(d2);
+            if (m2 <= best.d2) {
+                const unsigned c2 = __ballot_sync(FULL, d2 == m2);
+                int o = 0x7fffffff;
+                if ((c2 >> lane) & 1u) o = __ldg(&S.lorig[s]);
+                const int omin = (__popc(c2) == 1) ? __shfl_sync(FULL, o, __ffs(c2) - 1) : warp_min_int(o);
+                if (m2 < best.d2 || omin < best.prim) {
+                    best.d2 = m2;
+                    best.prim = omin;
+                }
+            }
+        } else {
+            wdescend<D, L - 1>(S, q, node * 32, tol2, best, wk);
+        }
+    }
+}
+
+template <int D>
+__device__ __forceinline__ Hit wquery(const SceneView &S, const float *q, Hit best, Work &wk) {
+    const float tol2 = prune_tol2<D>(S, q);
+    wk.nq += 1;
+    switch (S.wt_levels) {
+        case 1: wdescend<D, 1>(S, q, 0, tol2, best, wk); break;
+        case 2: wdescend<D, 2>(S, q, 0, tol2, best, wk); break;
+        case 3: wdescend<D, 3>(S, q, 0, tol2, best, wk); break;
+        case 4: wdescend<D, 4>(S, q, 0, tol2, best, wk); break;
+        default: wdescend<D, 5>(S, q, 0, tol2, best, wk); break;
+    }
+    return best;
+}
+
 // ------------------------------------------------------------------ records
 // Closest-point record at x for primitive prim (include/scene.cuh:180-223).
 struct Rec {
     float p[3];
     float n[3];
     float t0, t1;  // 2D: (h, 0); 3D: (w_b, w_c)
+    bool flip;     // the normal was negated to face the query point
 };
+
+// Per-walk boundary record stored by the forward pass for the adjoint:
+// code = -1 (invalid walk) or prim | (flip << 30); t0, t1 as float bits.
+struct WalkRec {
+    int code;
+    float t0, t1;
+};
+__host__ __device__ constexpr int walkrec_words(int D) { return D == 2 ? 2 : 4; }
 
 template <int D>
 __device__ __forceinline__ Rec closest_record(const SceneView &S, const float *x, int prim) {
@@ -402,7 +535,8 @@ __device__ __forceinline__ Rec closest_record(const SceneView &S, const float *x
         const float len = sqrtf(dot2(nx, ny, nx, ny));
         nx = nx / len;
         ny = ny / len;
-        if (!(dot2(nx, ny, pax, pay) > 0.0f)) {
+        r.flip = !(dot2(nx, ny, pax, pay) > 0.0f);
+        if (r.flip) {
             nx = -nx;
             ny = -ny;
         }
@@ -426,12 +560,49 @@ __device__ __forceinline__ Rec closest_record(const SceneView &S, const float *x
         ny = ny / len;
         nz = nz / len;
         const float axx = x[0] - t0.x, axy = x[1] - t0.y, axz = x[2] - t0.z;
-        const float sg = dot3(nx, ny, nz, axx, axy, axz) > 0.0f ? 1.0f : -1.0f;
+        r.flip = !(dot3(nx, ny, nz, axx, axy, axz) > 0.0f);
+        const float sg = r.flip ? -1.0f : 1.0f;
         r.n[0] = sg * nx;
         r.n[1] = sg * ny;
         r.n[2] = sg * nz;
         r.t0 = v;
         r.t1 = w;
+    }
+    return r;
+}
+
+// The record of closest_record() rebuilt from (prim, t0, t1, flip): the same
+// operations on the same inputs, so the same bits.
+template <int D>
+__device__ __forceinline__ Rec record_from(const SceneView &S, int prim, float t0, float t1, bool flip) {
+    Rec r;
+    r.flip = flip;
+    r.t0 = t0;
+    r.t1 = t1;
+    if (D == 2) {
+        const float4 s = __ldg(&S.seg[prim]);
+        r.p[0] = fmaf(s.z, t0, s.x);
+        r.p[1] = fmaf(s.w, t0, s.y);
+        r.p[2] = 0.0f;
+        float nx = s.w, ny = -s.z;
+        const float len = sqrtf(dot2(nx, ny, nx, ny));
+        nx = nx / len;
+        ny = ny / len;
+        r.n[0] = flip ? -nx : nx;
+        r.n[1] = flip ? -ny : ny;
+        r.n[2] = 0.0f;
+    } else {
+        const float4 a = __ldg(&S.tri[3 * prim]), b = __ldg(&S.tri[3 * prim + 1]), c = __ldg(&S.tri[3 * prim + 2]);
+        r.p[0] = fmaf(c.x, t1, fmaf(b.x, t0, a.x));
+        r.p[1] = fmaf(c.y, t1, fmaf(b.y, t0, a.y));
+        r.p[2] = fmaf(c.z, t1, fmaf(b.z, t0, a.z));
+        float nx, ny, nz;
+        cross3(b.x, b.y, b.z, c.x, c.y, c.z, nx, ny, nz);
+        const float len = sqrtf(dot3(nx, ny, nz, nx, ny, nz));
+        const float sg = flip ? -1.0f : 1.0f;
+        r.n[0] = sg * (nx / len);
+        r.n[1] = sg * (ny / len);
+        r.n[2] = sg * (nz / len);
     }
     return r;
 }
@@ -548,19 +719,26 @@ __device__ __forceinline__ float source(const SceneView &S, float x, float y, fl
     return 0.0f;
 }
 
-// Radius sample from the G CDF (include/wos.cuh:49-75); cdf may point to
-// shared memory.
-__device__ __forceinline__ float sample_G_radius(const float *cdf, int n, float u, float R, float &pdf) {
-    int l = 0, r = n - 1;
+// Radius sample from the G CDF (include/wos.cuh:49-75).  The guide table
+// (usually in shared memory) brackets the search; the bracket is checked and
+// widened when it does not hold, so the result is always the first l with
+// u < cdf[l], as a search over the whole table gives.
+__device__ __forceinline__ float sample_G_radius(const float *cdf, int n, const unsigned short *guide, int ng,
+                                                 float u, float R, float &pdf) {
+    int k = (int)(u * (float)ng);
+    k = min(max(k, 0), ng - 1);
+    int l = guide[k], r = guide[k + 1];
+    if (l > 0 && !(u >= __ldg(&cdf[l - 1]))) l = 0;
+    if (!(u < __ldg(&cdf[r]))) r = n - 1;
     while (l < r) {
         const int mid = (l + r) >> 1;
-        if (u < cdf[mid])
+        if (u < __ldg(&cdf[mid]))
             r = mid;
         else
             l = mid + 1;
     }
-    const float pmf = l == 0 ? cdf[0] : cdf[l] - cdf[l - 1];
-    const float prev = l == 0 ? 0.0f : cdf[l - 1];
+    const float pmf = l == 0 ? __ldg(&cdf[0]) : __ldg(&cdf[l]) - __ldg(&cdf[l - 1]);
+    const float prev = l == 0 ? 0.0f : __ldg(&cdf[l - 1]);
     u = (u - prev) / pmf;
     pdf = pmf * (float)n / R;
     return R * ((float)l + u) / (float)n;
@@ -569,11 +747,11 @@ __device__ __forceinline__ float sample_G_radius(const float *cdf, int n, float 
 // Interior source term of one step (include/wos.cuh:115-139 with the
 // importance-sampled branch of :121-130): returns the factor K with
 // contrib += f(y) * K, and y.
-__device__ __forceinline__ float source_step(const SceneView &S, const float *cdf, bool use_IS, float px, float py,
-                                             float d, uint32_t ra, uint32_t rb, float &yx, float &yy) {
+__device__ __forceinline__ float source_step(const SceneView &S, const unsigned short *guide, bool use_IS, float px,
+                                             float py, float d, uint32_t ra, uint32_t rb, float &yx, float &yy) {
     float dx, dy, pdf, weight;
     if (use_IS) {
-        const float rad = sample_G_radius(cdf, S.n_cdf, wosm::u01(ra), d, pdf);
+        const float rad = sample_G_radius(S.cdf, S.n_cdf, guide, S.n_guide, wosm::u01(ra), d, pdf);
         float s, c;
         wosm::sincos_2pi(wosm::u01(rb), &s, &c);
         pdf = pdf / wosm::kTwoPi;

@@ -117,6 +117,19 @@ SIGNATURES = {
         _I,
         [_P, _P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams), _P, _P, _P, _P, _P, _S, _P],
     ),
+    "wos_walk_record_bytes": (_S, [_I]),
+    "wos_solve_records": (_I, [_P, _P, _I, ctypes.POINTER(WosParams), _P, _P, _P, _P, _P, _S, _P]),
+    "wos_adjoint_records": (
+        _I,
+        [_P, _P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams), _P, _P, _P, _P, _P, _P, _P, _S,
+         _P],
+    ),
+    "wos_solve_adjoint_workspace_size": (_S, [_P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams)]),
+    "wos_solve_adjoint": (
+        _I,
+        [_P, _P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams), _I, _P, _P, _P, _P, _P, _P, _P,
+         _P, _S, _P],
+    ),
     "wos_set_work_counting": (_I, [_I]),
     "wos_work_counters": (_I, [_I, ctypes.POINTER(ctypes.c_int64)]),
     "wos_set_launch_config": (_I, [_I, ctypes.POINTER(WosLaunchConfig)]),

@@ -222,6 +222,69 @@ class NativeScene:
                  workspace.data_ptr(), need, stream())
         return (mean, var) if want_var else mean
 
+    def solve_records(self, P, s: WalkSettings, want_dcontrib=False, want_var=False,
+                      workspace: torch.Tensor | None = None):
+        """solve() that keeps each walk's boundary record (and, optionally, its
+        source-parameter derivative) for adjoint_records()."""
+        P = as_cuda(P, torch.float32, self.dim)
+        n = int(P.shape[0])
+        d = self.device
+        mean = torch.empty(n, dtype=torch.float64, device=d)
+        var = torch.empty(n, dtype=torch.float64, device=d) if want_var else None
+        rb = _lib.lib().wos_walk_record_bytes(self.dim)
+        rec = torch.empty(max(n * s.nwalks * rb, 1), dtype=torch.uint8, device=d)
+        dc = torch.empty(max(n * s.nwalks * 5, 1), dtype=torch.float32, device=d) if want_dcontrib else None
+        if n:
+            c = s.c()
+            need = _lib.lib().wos_solve_workspace_size(n, ctypes.byref(c))
+            if workspace is None or workspace.numel() < need:
+                workspace = torch.empty(need, dtype=torch.uint8, device=d)
+            call("wos_solve_records", self.h, P.data_ptr(), n, ctypes.byref(c), mean.data_ptr(), _ptr(var),
+                 rec.data_ptr(), _ptr(dc), workspace.data_ptr(), need, stream())
+        return mean, var, rec, dc
+
+    def adjoint_records(self, P, s: WalkSettings, a: AdjointSettings, dLdu, rec, dc,
+                        workspace: torch.Tensor | None = None):
+        P = as_cuda(P, torch.float32, self.dim)
+        dLdu = as_cuda(dLdu, torch.float32).reshape(-1)
+        n = int(P.shape[0])
+        d = self.device
+        dV = torch.zeros((self.nV, self.dim), dtype=torch.float32, device=d) if a.want_dV else None
+        dg = torch.zeros(self.nV, dtype=torch.float32, device=d) if a.want_dg else None
+        ds = torch.zeros(5, dtype=torch.float32, device=d) if a.want_dsrc else None
+        if n:
+            c, ca = s.c(), a.c()
+            need = _lib.lib().wos_adjoint_workspace_size(self.h)
+            if workspace is None or workspace.numel() < need:
+                workspace = torch.empty(need, dtype=torch.uint8, device=d)
+            call("wos_adjoint_records", self.h, P.data_ptr(), n, ctypes.byref(c), ctypes.byref(ca), dLdu.data_ptr(),
+                 rec.data_ptr(), _ptr(dc), _ptr(dV), _ptr(dg), _ptr(ds), workspace.data_ptr(), need, stream())
+        return dV, dg, ds
+
+    def solve_adjoint(self, P, s: WalkSettings, a: AdjointSettings, loss_kind=1, target=None, want_var=False,
+                      workspace: torch.Tensor | None = None):
+        """Fused forward + adjoint of a pointwise loss of the means (loss_kind
+        1: mean(u^2), 2: mean((u - target)^2), 0: target holds dL/du)."""
+        P = as_cuda(P, torch.float32, self.dim)
+        n = int(P.shape[0])
+        d = self.device
+        tg = as_cuda(target, torch.float32).reshape(-1) if target is not None else None
+        mean = torch.empty(n, dtype=torch.float64, device=d)
+        var = torch.empty(n, dtype=torch.float64, device=d) if want_var else None
+        loss = torch.zeros(1, dtype=torch.float64, device=d)
+        dV = torch.zeros((self.nV, self.dim), dtype=torch.float32, device=d) if a.want_dV else None
+        dg = torch.zeros(self.nV, dtype=torch.float32, device=d) if a.want_dg else None
+        ds = torch.zeros(5, dtype=torch.float32, device=d) if a.want_dsrc else None
+        if n:
+            c, ca = s.c(), a.c()
+            need = _lib.lib().wos_solve_adjoint_workspace_size(self.h, n, ctypes.byref(c), ctypes.byref(ca))
+            if workspace is None or workspace.numel() < need:
+                workspace = torch.empty(need, dtype=torch.uint8, device=d)
+            call("wos_solve_adjoint", self.h, P.data_ptr(), n, ctypes.byref(c), ctypes.byref(ca), int(loss_kind),
+                 _ptr(tg), mean.data_ptr(), _ptr(var), loss.data_ptr(), _ptr(dV), _ptr(dg), _ptr(ds),
+                 workspace.data_ptr(), need, stream())
+        return dict(mean=mean, var=var, loss=loss, dV=dV, dg=dg, dsrc=ds)
+
     def normal_derivative(self, rec, s: WalkSettings, a: AdjointSettings) -> torch.Tensor:
         valid = as_cuda(rec["valid"], torch.uint8).reshape(-1)
         n = int(valid.numel())

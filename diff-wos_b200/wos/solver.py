@@ -4,9 +4,12 @@
 `walk(p, scene, seed)` returns per-point means over nwalks walks as a torch
 float32 tensor.  When scene tensors (vertices, values, source_params) require
 grad, the result is attached to them through one torch.autograd.Function
-whose backward runs the adjoint kernel with the same seed: walks are
-recomputed from their Philox counters (common random numbers), never stored
--- the reference's _CustomSolver.backward (wos/solver.py:109-114).
+whose backward runs the adjoint kernel with the same seed -- the reference's
+_CustomSolver.backward (wos/solver.py:109-114).  Walks are defined by their
+Philox counters (common random numbers): the backward either repeats the
+primal walks or, when forward and backward walk the same way, starts from the
+boundary records the forward kept (8-16 bytes per walk); both give the same
+gradients.
 """
 from __future__ import annotations
 
@@ -141,13 +144,28 @@ def _record(scene, o):
 
 
 class _Job:
-    def __init__(self, fwd, bwd, p, scene, seed):
+    """One differentiable walk: forward values from `fwd`, gradients from
+    `bwd` with the same seed.  When both solvers walk with identical settings
+    the forward keeps every walk's boundary record and the backward starts
+    from it instead of repeating the primal walk (same result)."""
+
+    def __init__(self, fwd, bwd, p, scene, seed, needs=(True, True, True)):
         self.fwd, self.bwd, self.scene, self.seed = fwd, bwd, scene, seed
         self.P = points(p, scene.dim)
+        self.records = None
+        self.needs = needs
 
     def forward(self):
         if self.fwd is None:
             return torch.zeros(self.P.shape[0], dtype=torch.float32, device=self.P.device)
+        sf = self.fwd.walk_settings(self.scene, self.seed)
+        sb = self.bwd.walk_settings(self.scene, self.seed)
+        if sf == sb:
+            a = self.bwd.adjoint_settings(self.scene, *self.needs)
+            want_dc = bool(a.want_dsrc and sb.include_source and self.scene.source_type != 0 and self.scene.dim == 2)
+            mean, _, rec, dc = self.scene._native.solve_records(self.P, sf, want_dcontrib=want_dc)
+            self.records = (rec, dc)
+            return mean.to(torch.float32)
         return self.fwd.solve(self.P, self.scene, self.seed)
 
     def backward(self, grad, need_V, need_g, need_s):
@@ -155,7 +173,13 @@ class _Job:
         a = self.bwd.adjoint_settings(self.scene, need_V, need_g, need_s)
         if not (a.want_dV or a.want_dg or a.want_dsrc):
             return None, None, None
-        dV, dg, ds = self.scene._native.adjoint(self.P, s, a, grad.to(torch.float32).contiguous())
+        g = grad.to(torch.float32).contiguous()
+        if self.records is not None and (self.records[1] is not None or not a.want_dsrc or
+                                         not (s.include_source and self.scene.source_type != 0)):
+            dV, dg, ds = self.scene._native.adjoint_records(self.P, s, a, g, *self.records)
+        else:
+            dV, dg, ds = self.scene._native.adjoint(self.P, s, a, g)
+        self.records = None
         if ds is not None and self.scene.source_params is None:
             ds = None
         return dV, dg, ds
@@ -182,7 +206,8 @@ class _WalkFunction(torch.autograd.Function):
 def _attach(fwd, bwd, p, scene, seed):
     tensors = (scene.vertices, scene.values, scene.source_params_tensor())
     if torch.is_grad_enabled() and any(t.requires_grad for t in tensors):
-        return _WalkFunction.apply(_Job(fwd, bwd, p, scene, seed), *tensors)
+        needs = tuple(bool(t.requires_grad) for t in tensors)
+        return _WalkFunction.apply(_Job(fwd, bwd, p, scene, seed, needs), *tensors)
     if fwd is None:
         return torch.zeros(points(p, scene.dim).shape[0], dtype=torch.float32, device=scene.vertices.device)
     return fwd.solve(p, scene, seed)

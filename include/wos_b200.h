@@ -225,6 +225,43 @@ WOS_API int wos_adjoint(wos_scene_t scene, const float *P, int n, const wos_para
                 const float *dLdu, float *dV, float *dg, float *dsrc, void *workspace, size_t workspace_bytes,
                 wos_stream_t stream);
 
+/* ---------------------------------------------------------------- fused */
+
+/* Bytes of one per-walk boundary record (8 in 2D, 16 in 3D). */
+WOS_API size_t wos_walk_record_bytes(int dim);
+
+/* wos_solve that also stores each walk's boundary record into `records`
+ * (n * nwalks * wos_walk_record_bytes(dim) bytes, device) and, if dcontrib is
+ * not NULL, the derivative of its source term with respect to the 5 source
+ * parameters (n * nwalks * 5 floats), for a later wos_adjoint_records. */
+WOS_API int wos_solve_records(wos_scene_t scene, const float *P, int n, const wos_params *p, double *mean, double *var,
+                              void *records, float *dcontrib, void *workspace, size_t workspace_bytes,
+                              wos_stream_t stream);
+
+/* wos_adjoint that starts each sample from the record its primal walk left in
+ * wos_solve_records (same P, n and params) instead of walking it again --
+ * the reference recomputes the primal walk from the seed
+ * (wos/solver.py:109-114); the records make that recomputation unnecessary
+ * and the result is the same. */
+WOS_API int wos_adjoint_records(wos_scene_t scene, const float *P, int n, const wos_params *p,
+                                const wos_adjoint_params *a, const float *dLdu, const void *records,
+                                const float *dcontrib, float *dV, float *dg, float *dsrc, void *workspace,
+                                size_t workspace_bytes, wos_stream_t stream);
+
+WOS_API size_t wos_solve_adjoint_workspace_size(wos_scene_t scene, int n, const wos_params *p,
+                                                const wos_adjoint_params *a);
+
+/* Fused forward + adjoint step for a pointwise loss of the per-point means:
+ * wos_solve_records, the loss and dL/du, then wos_adjoint_records, in one
+ * call (one stream, no host round trip).  loss_kind 1: L = mean(u^2);
+ * 2: L = mean((u - target)^2) with target = target_or_dLdu (n floats);
+ * 0: dL/du given in target_or_dLdu.  loss (1 double, may be NULL) receives L
+ * (kinds 1, 2).  Gradients are added to dV / dg / dsrc (float32). */
+WOS_API int wos_solve_adjoint(wos_scene_t scene, const float *P, int n, const wos_params *p,
+                              const wos_adjoint_params *a, int loss_kind, const float *target_or_dLdu, double *mean,
+                              double *var, double *loss, float *dV, float *dg, float *dsrc, void *workspace,
+                              size_t workspace_bytes, wos_stream_t stream);
+
 /* ---------------------------------------------------------------- kernels */
 
 /* Launch shape of the persistent walk kernels: threads per block, blocks per

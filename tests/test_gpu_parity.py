@@ -240,3 +240,80 @@ def test_adjoint_matches_oracle(cuda, oracle, kind, src):
 def test_device_status_clean(cuda):
     import wos
     assert wos.device_status(reset=False) == 0
+
+
+# ---------------------------------------------------------------- fused path
+@pytest.mark.parametrize("kind,src", [("circle", None), ("star", (2, [0.0, 0.0, 0.0, 0.0, 1.0])),
+                                      ("sphere", None)])
+def test_fused_solve_adjoint_matches_oracle(cuda, oracle, kind, src):
+    from wos.native import AdjointSettings
+    if kind == "star":
+        V, F, g = star_scene(512)
+        ns, os_ = _scenes(oracle, V, F, g, *src)
+    else:
+        V, F, g = {"circle": lambda: circle_scene(256), "sphere": lambda: sphere_scene(2)}[kind]()
+        ns, os_ = _scenes(oracle, V, F, g)
+    P = _pts2(150, 12, -0.5, 0.5) if V.shape[1] == 2 else _pts3(120, 12, -0.5, 0.5)
+    s = _settings(nwalks=8, nsteps=64, seed=77, include_source=src is not None, use_IS_for_greens=src is not None)
+    a = AdjointSettings(epsilon2=1e-3, clamping=0.1, want_dV=True, want_dg=True, want_dsrc=src is not None)
+    out = ns.solve_adjoint(P, s, a, loss_kind=1)
+    ov, _, _ = os_.walk_values(P, _oparams(oracle, s))
+    om, _ = oracle.reduce(ov)
+    np.testing.assert_allclose(_np(out["mean"]), om, rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(_np(out["loss"])[0], (om ** 2).mean(), rtol=1e-10)
+    dLdu = (2.0 * _np(out["mean"]) / len(P)).astype(np.float32)
+    oa = oracle.make_adj(1e-3, 0.1, True, True, 1e-3, True, True, src is not None)
+    odV, odg, ods = os_.adjoint(P, _oparams(oracle, s), oa, dLdu)
+    np.testing.assert_allclose(_np(out["dV"]), odV, rtol=GRAD_RTOL, atol=GRAD_RTOL * np.abs(odV).max())
+    np.testing.assert_allclose(_np(out["dg"]), odg, rtol=GRAD_RTOL, atol=GRAD_RTOL * np.abs(odg).max())
+    if src is not None:
+        np.testing.assert_allclose(_np(out["dsrc"]), ods, rtol=GRAD_RTOL, atol=GRAD_RTOL * np.abs(ods).max())
+
+
+def test_records_adjoint_equals_recomputed(cuda, oracle):
+    from wos.native import AdjointSettings
+    V, F, g = star_scene(1024)
+    ns, _ = _scenes(oracle, V, F, g, 2, [1.0, 2.0, 0.0, 0.5, 1.0])
+    P = _pts2(300, 13, -0.5, 0.5)
+    s = _settings(nwalks=16, nsteps=64, seed=5, include_source=True, use_IS_for_greens=True)
+    a = AdjointSettings(epsilon2=1e-3, clamping=0.1, want_dV=True, want_dg=True, want_dsrc=True)
+    mean, _, rec, dc = ns.solve_records(P, s, want_dcontrib=True)
+    assert np.array_equal(_np(mean), _np(ns.solve(P, s)))
+    dLdu = (2.0 / len(P)) * mean.float()
+    r1 = ns.adjoint_records(P, s, a, dLdu, rec, dc)
+    r2 = ns.adjoint(P, s, a, dLdu)
+    for x, y in zip(r1, r2):
+        np.testing.assert_allclose(_np(x), _np(y), rtol=1e-5, atol=1e-6 * np.abs(_np(y)).max())
+
+
+def test_autograd_custom_solver_matches_native(cuda, oracle):
+    import torch
+    import wos
+    from wos.native import AdjointSettings
+    V, F, g = star_scene(512)
+    src = [0.0, 0.0, 0.0, 0.0, 1.0]
+    P = _pts2(200, 14, -0.5, 0.5)
+    Vt = torch.tensor(V, device="cuda", requires_grad=True)
+    gt = torch.tensor(g, device="cuda", requires_grad=True)
+    st = torch.tensor(src, device="cuda", requires_grad=True)
+    scene = wos.Polyline(Vt, F, gt, source_type=2, source_params=st)
+    fwd = wos.WoSWithSourceCUDA(nwalks=16, nsteps=64, use_IS_for_greens=True)
+    bwd = wos.OursCUDA(nwalks=16, nsteps=64, epsilon=1e-3, epsilon2=1e-3, grad_values=True, grad_source=True,
+                       use_IS_for_greens=True)
+    u = wos.CustomSolver(fwd, bwd).walk(P, scene, seed=9)
+    (u * u).mean().backward()
+    ns = scene._native
+    s = fwd.walk_settings(scene, 9)
+    mean = ns.solve(P, s)
+    np.testing.assert_array_equal(_np(u), _np(mean.float()))
+    a = AdjointSettings(epsilon2=1e-3, clamping=0.1, want_dV=True, want_dg=True, want_dsrc=True)
+    dV, dg, ds = ns.adjoint(P, s, a, (2.0 / len(P)) * mean.float())
+    for x, y in ((Vt.grad, dV), (gt.grad, dg), (st.grad, ds)):
+        np.testing.assert_allclose(_np(x), _np(y), rtol=1e-5, atol=1e-6 * np.abs(_np(y)).max())
+    # the reference's default OursCUDA gives only the shape gradient
+    Vt.grad = None
+    gt.grad = None
+    st.grad = None
+    u2 = wos.CustomSolver(fwd, wos.OursCUDA(nwalks=16, nsteps=64, use_IS_for_greens=True)).walk(P, scene, seed=9)
+    (u2 * u2).mean().backward()
+    assert Vt.grad is not None and gt.grad is None and st.grad is None
