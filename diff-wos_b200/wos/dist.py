@@ -1,11 +1,15 @@
 """Multi-GPU helpers: one process per GPU, torch.distributed for plumbing.
 
-Query points x walks are independent, so a solve shards by contiguous point
-ranges with the scene (and its LBVH) replicated on every rank; the forward
-needs no exchange, the adjoint one sum-all-reduce of the gradient buffers
-(per-vertex dV, dg and the 5 source coefficients).
+A solve shards by walks: every rank runs walks [offset, offset + count) of
+every query point (Philox walk indices stay global, so the union over ranks
+is exactly the single-GPU set of walks) with the scene and its trees
+replicated.  The forward needs one weighted sum of per-point means, the
+adjoint one sum-all-reduce of the gradient buffers (dV, dg and the 5 source
+coefficients).  No kernel waits on another rank.
 """
 from __future__ import annotations
+
+import dataclasses
 
 import torch
 import torch.distributed as dist
@@ -25,7 +29,7 @@ def shard(n: int, rank: int, size: int) -> tuple[int, int]:
 
 
 def allreduce_sum_(tensors) -> None:
-    """In-place sum over ranks of every non-None tensor (one flat buffer)."""
+    """In-place sum over ranks of every non-None tensor (one flat float64 buffer)."""
     ts = [t for t in tensors if t is not None]
     rank, size = world()
     if size == 1 or not ts:
@@ -48,13 +52,30 @@ def max_over_ranks(x: float, device=None) -> float:
     return float(t.item())
 
 
-def sharded_adjoint(native_scene, P, settings, adjoint, dLdu):
-    """Adjoint over all points with this rank computing its shard; the
-    gradient buffers are summed across ranks.  Walk indices keep their global
-    point index, so results equal a single-GPU run up to summation order."""
+def _local(settings, rank, size):
+    a, b = shard(int(settings.nwalks), rank, size)
+    return dataclasses.replace(settings, walk_offset=int(settings.walk_offset) + a, nwalks=b - a), b - a
+
+
+def sharded_solve(native_scene, P, settings):
+    """Per-point means over all nwalks walks, this rank running its share."""
     rank, size = world()
-    n = P.shape[0]
-    a, b = shard(n, rank, size)
-    dV, dg, ds = native_scene.adjoint_range(P, settings, adjoint, dLdu, a, b)
+    local, count = _local(settings, rank, size)
+    if count > 0:
+        mean = native_scene.solve(P, local) * (count / settings.nwalks)
+    else:
+        mean = torch.zeros(P.shape[0], dtype=torch.float64, device=P.device)
+    allreduce_sum_([mean])
+    return mean
+
+
+def sharded_adjoint(native_scene, P, settings, adjoint, dLdu):
+    """Gradients of sum_i dLdu[i] mean_i over all walks, this rank running its share."""
+    rank, size = world()
+    local, count = _local(settings, rank, size)
+    if count > 0:
+        dV, dg, ds = native_scene.adjoint(P, local, adjoint, dLdu * (count / settings.nwalks))
+    else:
+        dV, dg, ds = native_scene.adjoint(P, dataclasses.replace(settings, nwalks=1), adjoint, dLdu * 0.0)
     allreduce_sum_([dV, dg, ds])
     return dV, dg, ds
