@@ -130,6 +130,7 @@ SIGNATURES = {
         [_P, _P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams), _I, _P, _P, _P, _P, _P, _P, _P,
          _P, _S, _P],
     ),
+    "wos_solve_noalloc": (_I, [_P, _P, _I, ctypes.POINTER(WosParams), _P, _P, _P]),
     "wos_set_work_counting": (_I, [_I]),
     "wos_work_counters": (_I, [_I, ctypes.POINTER(ctypes.c_int64)]),
     "wos_set_launch_config": (_I, [_I, ctypes.POINTER(WosLaunchConfig)]),

@@ -262,6 +262,28 @@ WOS_API int wos_solve_adjoint(wos_scene_t scene, const float *P, int n, const wo
                               double *var, double *loss, float *dV, float *dg, float *dsrc, void *workspace,
                               size_t workspace_bytes, wos_stream_t stream);
 
+/* ---------------------------------------------------------------- no allocation */
+
+/* Largest n * nwalks that wos_solve_noalloc accepts. */
+#define WOS_NOALLOC_MAX_WALKS 4194304
+
+/* wos_solve without any device allocation, for callers that may not
+ * allocate device memory (applications that own the device through their
+ * own pool and forbid plug-ins from calling cudaMalloc, latency-critical
+ * loops that cannot take its implicit synchronisation, processes under a
+ * hard device-memory quota).  No counterpart in the reference.
+ *
+ * Scratch is a fixed array inside the library: 16 MiB + 256 bytes on every
+ * GPU that loads it, held until the process exits.  n * nwalks must not
+ * exceed WOS_NOALLOC_MAX_WALKS; larger requests fail with WOS_ERR_WORKSPACE
+ * and a message (split the points, or use wos_solve).  The first call on a
+ * device looks up the array's device address with that device current; make
+ * that first call before any stream capture.  All calls share the one
+ * array, so calls that overlap on the GPU (concurrent streams or threads)
+ * race on it: order them on one stream.  Results equal wos_solve's. */
+WOS_API int wos_solve_noalloc(wos_scene_t scene, const float *P, int n, const wos_params *p, double *mean, double *var,
+                              wos_stream_t stream);
+
 /* ---------------------------------------------------------------- kernels */
 
 /* Launch shape of the persistent walk kernels: threads per block, blocks per
