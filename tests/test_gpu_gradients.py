@@ -1,0 +1,100 @@
+"""Gradients of the fused forward + adjoint step against central finite
+differences with common random numbers (the reference's FD pattern,
+diff_solve/runner.py:111-136), on the 2D differentiable-solve workload
+(star polyline, f = 1 sampled with the G CDF, loss = mean(u^2)).
+
+Dirichlet values and the source offset enter each walk linearly without
+changing the walks, so their finite differences must match the adjoint to
+float rounding.  Vertex positions move the walks; there the adjoint and the
+FD estimate are compared through their seed-to-seed standard errors
+(north_star: within 2 standard errors).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SRC = [0.0, 0.0, 0.0, 0.0, 1.0]
+
+
+def _setup(nseg=1024, grid=96):
+    from wos import shapes
+    V, F = shapes.star(nseg)
+    g = (np.sin(3 * V[:, 0]) * np.cos(2 * V[:, 1])).astype(np.float32)
+    P = shapes.grid(grid)
+    P = P[shapes.inside_star(P, margin=0.01)]
+    return V, F, g, P
+
+
+def _settings(seed, nwalks=128):
+    from wos.native import WalkSettings
+    return WalkSettings(nwalks=nwalks, nsteps=64, epsilon=1e-3, use_IS_for_greens=True, include_source=True,
+                        seed=seed)
+
+
+def _adj():
+    from wos.native import AdjointSettings
+    return AdjointSettings(epsilon2=1e-3, clamping=0.1, want_dV=True, want_dg=True, want_dsrc=True)
+
+
+def _loss(V, F, g, src, P, seed, nwalks=128):
+    from wos.native import NativeScene
+    sc = NativeScene(V, F, g, 2, src)
+    m = sc.solve(P, _settings(seed, nwalks))
+    return float((m * m).mean())
+
+
+def test_values_and_source_gradients_match_fd(cuda):
+    from wos.native import NativeScene
+    V, F, g, P = _setup()
+    seed = 5
+    sc = NativeScene(V, F, g, 2, SRC)
+    out = sc.solve_adjoint(P, _settings(seed), _adj(), loss_kind=1)
+    dg = out["dg"].cpu().numpy()
+    ds = out["dsrc"].cpu().numpy()
+    rng = np.random.default_rng(0)
+    h = 1e-2  # the loss is quadratic in g: central differences are exact up to rounding
+    for k in rng.choice(len(V), 8, replace=False):
+        gp, gm = g.copy(), g.copy()
+        gp[k] += h
+        gm[k] -= h
+        fd = (_loss(V, F, gp, SRC, P, seed) - _loss(V, F, gm, SRC, P, seed)) / (2 * h)
+        assert abs(fd - dg[k]) <= 2e-3 * max(abs(fd), 1e-6) + 1e-7, (k, fd, dg[k])
+    # offset (index 4) and amplitude (index 3) of f = amp sin(A x + B y + C) + offset
+    for i in (3, 4):
+        sp, sm = list(SRC), list(SRC)
+        sp[i] += h
+        sm[i] -= h
+        fd = (_loss(V, F, g, sp, P, seed) - _loss(V, F, g, sm, P, seed)) / (2 * h)
+        assert abs(fd - ds[i]) <= 2e-3 * max(abs(fd), 1e-6) + 1e-7, (i, fd, ds[i])
+
+
+@pytest.mark.slow
+def test_vertex_gradients_match_fd_within_standard_errors(cuda):
+    from wos.native import NativeScene
+    V, F, g, P = _setup(nseg=512, grid=64)
+    rng = np.random.default_rng(1)
+    ks = rng.choice(len(V), 16, replace=False)
+    dirs = rng.normal(size=(16, 2))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    seeds = list(range(100, 112))
+    h = 1e-3
+    adj = np.zeros((len(seeds), len(ks)))
+    fd = np.zeros((len(seeds), len(ks)))
+    for si, seed in enumerate(seeds):
+        sc = NativeScene(V, F, g, 2, SRC)
+        out = sc.solve_adjoint(P, _settings(seed, 256), _adj(), loss_kind=1)
+        dV = out["dV"].cpu().numpy()
+        for j, (k, d) in enumerate(zip(ks, dirs)):
+            adj[si, j] = dV[k] @ d
+            Vp, Vm = V.copy(), V.copy()
+            Vp[k] += h * d
+            Vm[k] -= h * d
+            fd[si, j] = (_loss(Vp, F, g, SRC, P, seed, 256) - _loss(Vm, F, g, SRC, P, seed, 256)) / (2 * h)
+    se = np.sqrt(adj.var(0, ddof=1) / len(seeds) + fd.var(0, ddof=1) / len(seeds))
+    z = (adj.mean(0) - fd.mean(0)) / np.maximum(se, 1e-12)
+    # within 2 standard errors for the large majority; none wildly off
+    assert np.mean(np.abs(z) < 2.0) >= 0.8, z
+    assert np.all(np.abs(z) < 4.0), z
