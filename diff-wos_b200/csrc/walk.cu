@@ -969,6 +969,21 @@ int set_work_counting(int enable) {
     return 0;
 }
 
+int work_counting_enabled() { return g_count_work; }
+
+AdjCfg make_adj_cfg(const wos_adjoint_params &a) {
+    AdjCfg c;
+    c.epsilon2 = a.epsilon2;
+    c.clamping = a.clamping;
+    c.control_variates = a.control_variates;
+    c.source_in_nd = a.source_in_normal_derivative;
+    c.ball_eps = a.ball_epsilon;
+    c.want_dV = a.want_dV;
+    c.want_dg = a.want_dg;
+    c.want_dsrc = a.want_dsrc;
+    return c;
+}
+
 WalkCfg make_cfg(const wos_params &p) {
     WalkCfg c;
     c.count = g_count_work;
@@ -1174,6 +1189,474 @@ int launch_add_f64(const double *src, float *dst, long long n, cudaStream_t st) 
     k_add_f64_to_f32<<<G, B, 0, st>>>(src, dst, n);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail_cuda(e, "k_add_f64_to_f32 launch");
+    return 0;
+}
+
+// ------------------------------------------------------------------ batched launch
+// Many (scene, query set) items in one persistent launch per dimension.  The
+// walk index space is the concatenation of every item's n x nwalks walks in
+// item order (scene-major), so warps move through the items together and each
+// scene's trees stay resident in L2 while its walks run.  Each lane carries
+// its item; the cooperative query serves one lane's item at a time.
+
+__device__ __forceinline__ int find_item(const BatchItemDev *__restrict__ items, int n_items, long long idx) {
+    int lo = 0, hi = n_items - 1;  // last item with walk_begin <= idx
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&items[mid].walk_begin) <= idx)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int find_item_point(const BatchItemDev *__restrict__ items, int n_items, int p) {
+    int lo = 0, hi = n_items - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&items[mid].point_begin) <= p)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int D>
+__device__ __forceinline__ Hit warp_queries_batch(const SceneView *__restrict__ views, bool active, int item,
+                                                  const float *x, int warm, Work &work) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    Hit mine{-1, INFINITY};
+    unsigned act = __ballot_sync(FULL, active);
+    while (act) {
+        const int j = __ffs(act) - 1;
+        act &= act - 1u;
+        float q[3];
+        q[0] = __shfl_sync(FULL, x[0], j);
+        q[1] = __shfl_sync(FULL, x[1], j);
+        q[2] = D == 3 ? __shfl_sync(FULL, x[2], j) : 0.0f;
+        const int wp = __shfl_sync(FULL, warm, j);
+        const int it = __shfl_sync(FULL, item, j);
+        const SceneView &Sj = views[it];
+        Hit best{-1, INFINITY};
+        if (wp >= 0) {
+            best.prim = wp;
+            best.d2 = prim_d2<D>(Sj, wp, q);
+        }
+        const Hit h = wquery<D>(Sj, q, best, work);
+        if (lane == j) mine = h;
+    }
+    return mine;
+}
+
+template <int D>
+__global__ void __launch_bounds__(512) k_walk_batch(const SceneView *__restrict__ views,
+                                                   const WalkCfg *__restrict__ cfgs,
+                                                   const BatchItemDev *__restrict__ items, int n_items,
+                                                   long long total, unsigned long long *counter, int chunk,
+                                                   WalkOut out, int count_work) {
+    Queue q{0, 0, false};
+    bool active = false;
+    long long idx = 0;
+    int item = 0;
+    uint32_t pt = 0, wk = 0;
+    Walker w;
+    w.last = -1;
+    Work work{0, 0, 0};
+    for (;;) {
+        const bool was = active;
+        if (!refill(q, active, idx, counter, total, chunk)) break;
+        if (active && !was) {
+            item = find_item(items, n_items, idx);
+            const BatchItemDev &it = items[item];
+            const long long local = idx - it.walk_begin;
+            pt = (uint32_t)(local / it.nwalks);
+            wk = cfgs[item].walk_offset + (uint32_t)(local - (long long)pt * it.nwalks);
+            w.start(it.P + (size_t)pt * D, D);
+        }
+        const Hit hit = warp_queries_batch<D>(views, active, item, w.p, w.last, work);
+        if (!active) continue;
+        const SceneView &S = views[item];
+        const WalkCfg &c = cfgs[item];
+        w.last = hit.prim;
+        const int r = walker_advance<D>(w, S, hit, c, c.eps, c.project != 0, c.prevent_fd != 0, pt, wk, ROLE_PRIMAL,
+                                        out.wds != nullptr, S.guide);
+        if (r == W_CONTINUE) continue;
+        active = false;
+        float v = 0.0f;
+        Rec rec;
+        if (r == W_VALID) {
+            rec = closest_record<D>(S, w.p, hit.prim);
+            v = dirichlet<D>(S, hit.prim, rec.t0, rec.t1, nullptr, nullptr);
+            if (c.include_source) v += w.contrib;
+            if (!isfinite(v)) atomicOr(&g_status, ST_NONFINITE);
+        }
+        out.values[idx] = v;
+        if (out.wrec) {
+            if (D == 2) {
+                reinterpret_cast<int2 *>(out.wrec)[idx] =
+                    r == W_VALID ? make_int2(hit.prim | (rec.flip ? 0x40000000 : 0), __float_as_int(rec.t0))
+                                 : make_int2(-1, 0);
+            } else {
+                reinterpret_cast<int4 *>(out.wrec)[idx] =
+                    r == W_VALID ? make_int4(hit.prim | (rec.flip ? 0x40000000 : 0), __float_as_int(rec.t0),
+                                             __float_as_int(rec.t1), 0)
+                                 : make_int4(-1, 0, 0, 0);
+            }
+        }
+        if (out.wds) {
+#pragma unroll
+            for (int k = 0; k < 5; ++k) out.wds[(size_t)idx * 5 + k] = r == W_VALID ? w.ds[k] : 0.0f;
+        }
+    }
+    if (count_work) flush_work<true>(work);
+}
+
+// Per-point FP64 mean / variance over the concatenated point space.
+__global__ void k_reduce_batch(const float *__restrict__ vals, const BatchItemDev *__restrict__ items, int n_items,
+                               int n_points, double *mean, double *var) {
+    const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (p >= n_points) return;
+    const int item = find_item_point(items, n_items, p);
+    const BatchItemDev &it = items[item];
+    const int nw = it.nwalks;
+    const float *v = vals + it.walk_begin + (long long)(p - it.point_begin) * nw;
+    double s = 0.0, cc = 0.0;
+    for (int w = lane; w < nw; w += 32) neumaier_add(s, cc, (double)v[w]);
+    const double m = warp_sum_comp(s, cc) / nw;
+    double qq = 0.0, qc = 0.0;
+    for (int w = lane; w < nw; w += 32) {
+        const double e = (double)v[w] - m;
+        neumaier_add(qq, qc, e * e);
+    }
+    const double q2 = warp_sum_comp(qq, qc);
+    if (lane == 0) {
+        mean[p] = m;
+        if (var) var[p] = nw > 1 ? q2 / (nw - 1) : 0.0;
+    }
+}
+
+// Per item: dL/du of its points and its loss (one block per item).
+__global__ void k_loss_batch(const double *__restrict__ mean, const BatchItemDev *__restrict__ items, float *dLdu,
+                             double *loss) {
+    __shared__ double red[256];
+    const BatchItemDev &it = items[blockIdx.x];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < it.n; i += blockDim.x) {
+        const int p = it.point_begin + i;
+        const double u = mean[p];
+        double e = u;
+        if (it.loss_kind == 2) e = u - (double)it.target[i];
+        if (it.loss_kind == 0) {
+            dLdu[p] = it.target[i];
+        } else {
+            dLdu[p] = (float)(2.0 * e / it.n);
+            acc += e * e / it.n;
+        }
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) loss[blockIdx.x] = red[0];
+}
+
+// Adjoint of every item, starting from the forward records.  Gradients go to
+// per-item FP64 accumulators (acc + it.dV_off / dg_off / ds_off).
+template <int D>
+__global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
+    const SceneView *__restrict__ views, const WalkCfg *__restrict__ cfgs, AdjCfg a,
+    const BatchItemDev *__restrict__ items, int n_items, long long total, const float *__restrict__ dLdu,
+    unsigned long long *counter, int chunk, const int *__restrict__ wrec, const float *__restrict__ wds, double *acc,
+    int count_work) {
+    extern __shared__ float4 smem[];
+    AdjSlot &slot = *reinterpret_cast<AdjSlot *>(reinterpret_cast<double *>(smem) + (size_t)threadIdx.x * ADJ_THREAD_WORDS);
+    double *acc_src = slot.acc;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) acc_src[k] = 0.0;
+    int acc_item = -1;  // item whose source gradient acc_src holds
+    NdState &st = slot.st;
+    float *rn = slot.rn;
+    float &rt0 = slot.rt0, &rt1 = slot.rt1;
+    float &ba = slot.ba, &bb = slot.bb;
+    int &bk = slot.bk;
+    Queue q{0, 0, false};
+    bool active = false;
+    long long idx = 0;
+    int item = 0;
+    uint32_t pt = 0, wk = 0;
+    int phase = PH_IDLE;
+    double W = 0.0;
+    Walker w;
+    int rprim = 0;
+    float qpos[3] = {0, 0, 0};
+    Work work{0, 0, 0};
+    w.last = -1;
+    for (;;) {
+        const bool was = active;
+        if (!refill(q, active, idx, counter, total, chunk)) break;
+        if (active && !was) {
+            item = find_item(items, n_items, idx);
+            const BatchItemDev &it = items[item];
+            const SceneView &S = views[item];
+            const WalkCfg &c = cfgs[item];
+            const long long local = idx - it.walk_begin;
+            pt = (uint32_t)(local / it.nwalks);
+            wk = c.walk_offset + (uint32_t)(local - (long long)pt * it.nwalks);
+            W = (double)__ldg(&dLdu[it.point_begin + pt]) / it.nwalks;
+            phase = PH_BALL;
+            int code = -1;
+            if (D == 2) {
+                const int2 wr = __ldg(reinterpret_cast<const int2 *>(wrec) + idx);
+                code = wr.x;
+                rt0 = __int_as_float(wr.y);
+                rt1 = 0.0f;
+            } else {
+                const int4 wr = __ldg(reinterpret_cast<const int4 *>(wrec) + idx);
+                code = wr.x;
+                rt0 = __int_as_float(wr.y);
+                rt1 = __int_as_float(wr.z);
+            }
+            if (W == 0.0 || code < 0) {
+                active = false;
+            } else {
+                rprim = code & 0x3fffffff;
+                const Rec rec = record_from<D>(S, rprim, rt0, rt1, (code & 0x40000000) != 0);
+                int vid[3];
+                float wts[3];
+                st.uref = dirichlet<D>(S, rprim, rt0, rt1, vid, wts);
+                if (a.want_dg) {
+#pragma unroll
+                    for (int s2 = 0; s2 < D; ++s2) atomicAdd(&acc[it.dg_off + vid[s2]], W * (double)wts[s2]);
+                }
+                if (wds != nullptr && a.want_dsrc && c.include_source && S.src_type != 0) {
+                    if (acc_item != item) {
+                        if (acc_item >= 0) {
+#pragma unroll
+                            for (int k = 0; k < 5; ++k)
+                                if (acc_src[k] != 0.0) atomicAdd(&acc[items[acc_item].ds_off + k], acc_src[k]);
+                        }
+#pragma unroll
+                        for (int k = 0; k < 5; ++k) acc_src[k] = 0.0;
+                        acc_item = item;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) acc_src[k] += W * (double)__ldg(&wds[(size_t)idx * 5 + k]);
+                }
+                if (!a.want_dV) {
+                    active = false;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < D; ++k) {
+                        st.p[k] = rec.p[k];
+                        rn[k] = rec.n[k];
+                    }
+                    ba = a.ball_eps;
+                    bb = S.half_min_extent;
+                    bk = 0;
+                    const float m = (ba + bb) * 0.5f;
+#pragma unroll
+                    for (int k = 0; k < D; ++k) qpos[k] = fmaf(rn[k], m, st.p[k]);
+                }
+            }
+        }
+        const bool walking = phase == PH_ANTI_WALK;
+        float x[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) x[k] = walking ? w.p[k] : qpos[k];
+        const Hit hit = warp_queries_batch<D>(views, active, item, x, walking ? w.last : rprim, work);
+        if (!active) continue;
+        const SceneView &S = views[item];
+        const WalkCfg &c = cfgs[item];
+        const bool with_src = a.source_in_nd && D == 2 && S.src_type != 0;
+        if (walking) w.last = hit.prim;
+        bool finish_anti = false;
+        float uq = 0.0f;
+        if (phase == PH_BALL) {
+            const float d = sqrtf(hit.d2);
+            const float m = (ba + bb) * 0.5f;
+            if (fabsf(d - m) < 1e-5f)
+                ba = m;
+            else
+                bb = m;
+            ++bk;
+            if (bk < 10) {
+                const float m2 = (ba + bb) * 0.5f;
+#pragma unroll
+                for (int k = 0; k < D; ++k) qpos[k] = fmaf(rn[k], m2, st.p[k]);
+                continue;
+            }
+            st.R = ba;
+#pragma unroll
+            for (int k = 0; k < D; ++k) st.n[k] = -rn[k];
+            if (D == 2) st.n[2] = 0.0f;
+            nd_setup<D>(st, S, c, a, pt, wk);
+            nd_point<D>(st, qpos);
+            phase = PH_ANTI_START;
+            continue;
+        }
+        const uint32_t role = st.which == 0 ? ROLE_ANTI_A : ROLE_ANTI_B;
+        if (phase == PH_ANTI_START) {
+            const float d = sqrtf(hit.d2);
+            if (d < a.epsilon2) {
+                const Rec r2 = closest_record<D>(S, qpos, hit.prim);
+                uq = dirichlet<D>(S, hit.prim, r2.t0, r2.t1, nullptr, nullptr);
+                finish_anti = true;
+            } else {
+                w.start(qpos, D);
+                w.last = hit.prim;
+                const int r = walker_advance<D>(w, S, hit, c, a.epsilon2, false, false, pt, wk, role, false, S.guide);
+                if (r == W_CONTINUE) {
+                    phase = PH_ANTI_WALK;
+                    continue;
+                }
+                if (r == W_VALID) {
+                    const Rec r2 = closest_record<D>(S, w.p, hit.prim);
+                    uq = dirichlet<D>(S, hit.prim, r2.t0, r2.t1, nullptr, nullptr);
+                    if (with_src) uq += w.contrib;
+                }
+                finish_anti = true;
+            }
+        } else {  // PH_ANTI_WALK
+            const int r = walker_advance<D>(w, S, hit, c, a.epsilon2, false, false, pt, wk, role, false, S.guide);
+            if (r == W_CONTINUE) continue;
+            if (r == W_VALID) {
+                const Rec r2 = closest_record<D>(S, w.p, hit.prim);
+                uq = dirichlet<D>(S, hit.prim, r2.t0, r2.t1, nullptr, nullptr);
+                if (with_src) uq += w.contrib;
+            }
+            finish_anti = true;
+        }
+        if (finish_anti) {
+            nd_accumulate<D>(st, a, uq);
+            st.which += 1;
+            if (st.which == 1) {
+                nd_point<D>(st, qpos);
+                phase = PH_ANTI_START;
+                continue;
+            }
+            float gn[3], gt[3];
+            nd_finish<D>(st, S, c, a, pt, wk, with_src, gn);
+            tangent_derivative<D>(S, rprim, gt);
+            int vid[3];
+            float wts[3];
+            dirichlet<D>(S, rprim, rt0, rt1, vid, wts);
+            const long long off = items[item].dV_off;
+#pragma unroll
+            for (int s2 = 0; s2 < D; ++s2)
+#pragma unroll
+                for (int k = 0; k < D; ++k)
+                    atomicAdd(&acc[off + (long long)vid[s2] * D + k], W * (double)(-(wts[s2] * (gn[k] + gt[k]))));
+            active = false;
+            phase = PH_IDLE;
+        }
+    }
+    if (count_work) flush_work<true>(work);
+    if (acc_item >= 0) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+            if (acc_src[k] != 0.0) atomicAdd(&acc[items[acc_item].ds_off + k], acc_src[k]);
+    }
+}
+
+__global__ void k_acc_to_f32(const double *__restrict__ acc, float *out, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = (float)acc[i];
+}
+
+template <typename Kern>
+static int persistent_grid(Kern kern, int block, size_t smem, int blocks_per_sm, int &grid) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)");
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, block, smem);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (occ < 1) return fail(WOS_ERR_UNSUPPORTED, "batch kernel does not fit on an SM with this launch config");
+    grid = sms * (blocks_per_sm > 0 ? std::min(blocks_per_sm, occ) : occ);
+    return 0;
+}
+
+int launch_walk_batch(int D, const SceneView *views, const WalkCfg *cfgs, const BatchItemDev *items, int n_items,
+                      long long total, const BatchLaunch &L, const WalkOut &out, unsigned long long *counter,
+                      cudaStream_t st) {
+    if (total == 0 || n_items == 0) return 0;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
+    int grid = 0;
+    if (D == 2) {
+        if (int rc = persistent_grid(k_walk_batch<2>, L.block, 0, L.blocks_per_sm, grid)) return rc;
+        k_walk_batch<2><<<grid, L.block, 0, st>>>(views, cfgs, items, n_items, total, counter, L.chunk, out,
+                                                  L.count_work);
+    } else {
+        if (int rc = persistent_grid(k_walk_batch<3>, L.block, 0, L.blocks_per_sm, grid)) return rc;
+        k_walk_batch<3><<<grid, L.block, 0, st>>>(views, cfgs, items, n_items, total, counter, L.chunk, out,
+                                                  L.count_work);
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_walk_batch launch");
+    return 0;
+}
+
+int launch_adjoint_batch(int D, const SceneView *views, const WalkCfg *cfgs, const AdjCfg &a,
+                         const BatchItemDev *items, int n_items, long long total, const float *dLdu,
+                         const int *wrec, const float *wds, double *acc, const BatchLaunch &L,
+                         unsigned long long *counter, cudaStream_t st) {
+    if (total == 0 || n_items == 0) return 0;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
+    const int block = std::min(L.block, 256);
+    const size_t smem = (size_t)block * ADJ_THREAD_WORDS * 8;
+    const int chunk = std::max(1, L.chunk / 2);
+    int grid = 0;
+    if (D == 2) {
+        if (int rc = persistent_grid(k_adjoint_batch<2>, block, smem, L.blocks_per_sm, grid)) return rc;
+        k_adjoint_batch<2><<<grid, block, smem, st>>>(views, cfgs, a, items, n_items, total, dLdu, counter, chunk,
+                                                      wrec, wds, acc, L.count_work);
+    } else {
+        if (int rc = persistent_grid(k_adjoint_batch<3>, block, smem, L.blocks_per_sm, grid)) return rc;
+        k_adjoint_batch<3><<<grid, block, smem, st>>>(views, cfgs, a, items, n_items, total, dLdu, counter, chunk,
+                                                      wrec, wds, acc, L.count_work);
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_adjoint_batch launch");
+    return 0;
+}
+
+int launch_reduce_batch(const float *vals, const BatchItemDev *items, int n_items, int n_points, double *mean,
+                        double *var, cudaStream_t st) {
+    if (n_points == 0) return 0;
+    const int B = 256;
+    const long long G = ((long long)n_points * 32 + B - 1) / B;
+    k_reduce_batch<<<(unsigned)G, B, 0, st>>>(vals, items, n_items, n_points, mean, var);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_reduce_batch launch");
+    return 0;
+}
+
+int launch_loss_batch(const double *mean, const BatchItemDev *items, int n_items, float *dLdu, double *loss,
+                      cudaStream_t st) {
+    if (n_items == 0) return 0;
+    k_loss_batch<<<n_items, 256, 0, st>>>(mean, items, dLdu, loss);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_loss_batch launch");
+    return 0;
+}
+
+int launch_acc_to_f32(const double *acc, float *out, long long n, cudaStream_t st) {
+    if (n == 0) return 0;
+    const int B = 256;
+    const int G = (int)std::min<long long>((n + B - 1) / B, 8192);
+    k_acc_to_f32<<<G, B, 0, st>>>(acc, out, n);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_acc_to_f32 launch");
     return 0;
 }
 

@@ -58,10 +58,39 @@ struct AdjOut {
 
 enum AdjMode { ADJ_RECOMPUTE = 0, ADJ_ND_ONLY = 1, ADJ_FROM_RECORDS = 2 };
 
+// One (scene, query set) item of a batched launch, in device memory.
+struct BatchItemDev {
+    const float *P;          // n x dim query points
+    long long walk_begin;    // first index of this item in the concatenated walk space
+    int n, nwalks;
+    int point_begin;         // first index in the concatenated point space
+    int loss_kind;           // 0: dL/du given, 1: mean(u^2), 2: mean((u - target)^2)
+    const float *target;     // n floats (kinds 0 and 2)
+    long long dV_off, dg_off, ds_off;  // offsets of its FP64 gradient accumulators
+};
+
+struct BatchLaunch {
+    int block, blocks_per_sm, chunk, count_work;
+};
+
 WalkCfg make_cfg(const wos_params &p);
+AdjCfg make_adj_cfg(const wos_adjoint_params &a);
+int launch_walk_batch(int D, const SceneView *views, const WalkCfg *cfgs, const BatchItemDev *items, int n_items,
+                      long long total, const BatchLaunch &L, const WalkOut &out, unsigned long long *counter,
+                      cudaStream_t st);
+int launch_adjoint_batch(int D, const SceneView *views, const WalkCfg *cfgs, const AdjCfg &a,
+                         const BatchItemDev *items, int n_items, long long total, const float *dLdu,
+                         const int *wrec, const float *wds, double *acc, const BatchLaunch &L,
+                         unsigned long long *counter, cudaStream_t st);
+int launch_reduce_batch(const float *vals, const BatchItemDev *items, int n_items, int n_points, double *mean,
+                        double *var, cudaStream_t st);
+int launch_loss_batch(const double *mean, const BatchItemDev *items, int n_items, float *dLdu, double *loss,
+                      cudaStream_t st);
+int launch_acc_to_f32(const double *acc, float *out, long long n, cudaStream_t st);
 int read_status(int reset, int *out);
 int read_work(int reset, unsigned long long *out);
 int set_work_counting(int enable);
+int work_counting_enabled();
 int set_launch_config(int dim, const wos_launch_config *cfg);
 int get_launch_config(int dim, wos_launch_config *out);
 

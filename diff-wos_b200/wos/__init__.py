@@ -7,6 +7,7 @@ CUDA tensors and every compute path runs in libwos_b200.so through its C ABI
 (include/wos_b200.h).  There is no CPU fallback.
 """
 from . import _lib, shapes
+from .batch import BatchItem, BatchPlan
 from ._lib import WosError, device_status, get_launch_config, set_launch_config, set_work_counting, work_counters
 from .scene import BoundarySamplingRecord, ClosestPointRecord, Detector, Intersection, Polyline
 from .scene3d import ClosestPointRecord3D, Detector3D, Detector3DY, Scene3D
@@ -23,5 +24,5 @@ __all__ = [
     "Detector", "Detector3D", "Detector3DY", "Intersection", "Ours", "Ours3D", "OursCUDA", "Polyline", "Sampler",
     "Scene3D", "Solver", "Statistics", "WoS", "WoS3D", "WoS3DCUDA", "WoSCUDA", "WoSWithSource", "WoSWithSourceCUDA",
     "Baseline", "WosError", "device_status", "get_launch_config", "set_launch_config", "set_work_counting",
-    "work_counters", "shapes",
+    "work_counters", "shapes", "BatchItem", "BatchPlan",
 ]

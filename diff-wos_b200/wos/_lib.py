@@ -84,6 +84,17 @@ class WosLaunchConfig(ctypes.Structure):
     ]
 
 
+class WosBatchItem(ctypes.Structure):
+    _fields_ = [
+        ("scene", ctypes.c_void_p),
+        ("P", ctypes.c_void_p),
+        ("n", ctypes.c_int32),
+        ("loss_kind", ctypes.c_int32),
+        ("target_or_dLdu", ctypes.c_void_p),
+        ("params", WosParams),
+    ]
+
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _F = ctypes.c_float
@@ -131,6 +142,16 @@ SIGNATURES = {
          _P, _S, _P],
     ),
     "wos_solve_noalloc": (_I, [_P, _P, _I, ctypes.POINTER(WosParams), _P, _P, _P]),
+    "wos_batch_create": (_I, [ctypes.POINTER(WosBatchItem), _I, ctypes.POINTER(WosAdjointParams), _I, _P,
+                              ctypes.POINTER(_P)]),
+    "wos_batch_set_launch": (_I, [_P, _I, _I, _I]),
+    "wos_batch_refresh": (_I, [_P, _P]),
+    "wos_batch_run": (_I, [_P, _I, _P]),
+    "wos_batch_outputs": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),
+    "wos_batch_copy_outputs": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _P]),
+    "wos_batch_info": (_I, [_P, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                            ctypes.POINTER(ctypes.c_int32)]),
+    "wos_batch_destroy": (_I, [_P, _P]),
     "wos_set_work_counting": (_I, [_I]),
     "wos_work_counters": (_I, [_I, ctypes.POINTER(ctypes.c_int64)]),
     "wos_set_launch_config": (_I, [_I, ctypes.POINTER(WosLaunchConfig)]),

@@ -262,6 +262,56 @@ WOS_API int wos_solve_adjoint(wos_scene_t scene, const float *P, int n, const wo
                               double *var, double *loss, float *dV, float *dg, float *dsrc, void *workspace,
                               size_t workspace_bytes, wos_stream_t stream);
 
+/* ---------------------------------------------------------------- batched */
+
+/* One (scene, query set) of a batch.  P (n x dim) and target_or_dLdu stay at
+ * their device addresses for the batch's lifetime (a captured graph reads
+ * them in place); their contents may change between runs.  loss_kind as in
+ * wos_solve_adjoint. */
+typedef struct wos_batch_item {
+    wos_scene_t scene;
+    const float *P;
+    int32_t n;
+    int32_t loss_kind;
+    const float *target_or_dLdu;
+    wos_params params;
+} wos_batch_item;
+
+typedef struct wos_batch_s *wos_batch_t;
+
+/* Plan a batched forward (+ adjoint if want_adjoint) over many items: items
+ * of one dimension run as one persistent work-queue launch per phase over the
+ * concatenation of their walks, in item order (order the items scene-major).
+ * Buffers for all outputs are owned by the plan (wos_batch_outputs).  This
+ * is the batched form of wos_solve_adjoint; no counterpart in the reference,
+ * whose callers loop over scenes with one thrust launch each
+ * (include/wos.cuh:407-440). */
+WOS_API int wos_batch_create(const wos_batch_item *items, int n_items, const wos_adjoint_params *a, int want_adjoint,
+                             wos_stream_t stream, wos_batch_t *out);
+
+/* Launch shape of the batch kernels (see wos_launch_config). */
+WOS_API int wos_batch_set_launch(wos_batch_t b, int block_threads, int blocks_per_sm, int chunk);
+
+/* Re-read the scenes' device views (after wos_scene_update_vertices). */
+WOS_API int wos_batch_refresh(wos_batch_t b, wos_stream_t stream);
+
+/* Run one step.  use_graph != 0: the step is captured once into a CUDA graph
+ * (on the first call) and replayed with one graph launch per call. */
+WOS_API int wos_batch_run(wos_batch_t b, int use_graph, wos_stream_t stream);
+
+/* Device pointers to item `item`'s outputs: per-point mean / var (double),
+ * its loss (double), gradients dV (nV x dim), dg (nV), dsrc (5) (float, NULL
+ * without adjoint).  Valid until wos_batch_destroy. */
+WOS_API int wos_batch_outputs(wos_batch_t b, int item, const double **mean, const double **var, const double **loss,
+                              const float **dV, const float **dg, const float **dsrc);
+
+/* Copy item `item`'s outputs into caller buffers (device; any may be NULL). */
+WOS_API int wos_batch_copy_outputs(wos_batch_t b, int item, double *mean, double *var, double *loss, float *dV,
+                                   float *dg, float *dsrc, wos_stream_t stream);
+
+WOS_API int wos_batch_info(wos_batch_t b, int64_t *total_walks, int64_t *total_points, int32_t *n_groups);
+WOS_API int wos_batch_destroy(wos_batch_t b, wos_stream_t stream);
+
 /* ---------------------------------------------------------------- no allocation */
 
 /* Largest n * nwalks that wos_solve_noalloc accepts. */
