@@ -156,3 +156,77 @@ def harmonic_c3(P):
     """x^2 - y^2 + z (harmonic)."""
     x, y, z = (P[:, k].astype(np.float64) for k in range(3))
     return x * x - y * y + z
+
+
+# ---------------------------------------------------------------- harmonic polynomials
+def harmonic_basis(P, degree: int):
+    """Harmonic polynomials of degree 1..degree at points P (2D or 3D), one
+    column each: Re/Im of (x + iy)^k in 2D; in 3D x, y, z, the degree-2
+    harmonics xy, yz, zx, x^2 - y^2, y^2 - z^2 and the degree-3 harmonics
+    xyz, x^3 - 3xy^2, y^3 - 3yz^2, z^3 - 3zx^2, x^3 - 3xz^2, y^3 - 3yx^2, z^3 - 3zy^2."""
+    P = np.asarray(P, np.float64)
+    if P.shape[1] == 2:
+        z = P[:, 0] + 1j * P[:, 1]
+        cols = []
+        for k in range(1, degree + 1):
+            w = z ** k
+            cols += [w.real, w.imag]
+        return np.stack(cols, 1)
+    x, y, zz = P[:, 0], P[:, 1], P[:, 2]
+    cols = [x, y, zz]
+    if degree >= 2:
+        cols += [x * y, y * zz, zz * x, x * x - y * y, y * y - zz * zz]
+    if degree >= 3:
+        cols += [x * y * zz, x ** 3 - 3 * x * y * y, y ** 3 - 3 * y * zz * zz, zz ** 3 - 3 * zz * x * x,
+                 x ** 3 - 3 * x * zz * zz, y ** 3 - 3 * y * x * x, zz ** 3 - 3 * zz * y * y]
+    return np.stack(cols, 1)
+
+
+def harmonic_poly(P, coeffs, degree):
+    return harmonic_basis(P, degree) @ np.asarray(coeffs, np.float64)
+
+
+# ---------------------------------------------------------------- batched workload
+def batched_scenes(seed: int = 0, n_stars: int = 128, n_spheres: int = 128, scale: float = 1.0,
+                   sphere_levels=(3, 4, 5, 6)):
+    """Seeded many-scene workload: random star polylines (256-16384 segments,
+    3-9 lobes, amplitude 0.1-0.3) and noise-displaced icospheres (1280-81920
+    triangles), each with 1k-200k query points (log-uniform, times `scale`)
+    and 16-256 walks (log-uniform), boundary data a harmonic polynomial of
+    degree 1-3 with coefficients in [-1, 1].  Returns dicts with V, F, g, the
+    point count, walks, and the polynomial (degree, coeffs) whose values are
+    the exact interior solution.  Query points are drawn by the caller
+    (see sample_box) so an exact inside test can filter them."""
+    rng = np.random.default_rng(seed)
+    base = {}
+    out = []
+    for i in range(n_stars + n_spheres):
+        is_star = i < n_stars
+        npts = int(round(np.exp(rng.uniform(np.log(1e3), np.log(2e5))) * scale))
+        nwalks = int(round(np.exp(rng.uniform(np.log(16), np.log(256)))))
+        deg = int(rng.integers(1, 4))
+        if is_star:
+            nseg = int(round(np.exp(rng.uniform(np.log(256), np.log(16384)))))
+            lobes = int(rng.integers(3, 10))
+            amp = float(rng.uniform(0.1, 0.3))
+            V, F = star(nseg, 0.6, amp, lobes, phase=float(rng.uniform(0, 2 * np.pi)))
+            ncoef = 2 * deg
+        else:
+            lvl = int(rng.choice(sphere_levels))
+            if lvl not in base:
+                base[lvl] = icosphere(lvl)
+            V0, F = base[lvl]
+            V = (V0.astype(np.float64) * (1.0 + 0.15 * value_noise3(V0.astype(np.float64), seed=1000 + i))[:, None])
+            V = V.astype(np.float32)
+            ncoef = {1: 3, 2: 8, 3: 15}[deg]
+        coeffs = rng.uniform(-1, 1, ncoef)
+        g = harmonic_poly(V, coeffs, deg).astype(np.float32)
+        out.append(dict(V=V, F=F, g=g, dim=V.shape[1], n=max(npts, 1), nwalks=nwalks, degree=deg, coeffs=coeffs,
+                        seed=int(rng.integers(0, 2 ** 31))))
+    return out
+
+
+def sample_box(V, n, rng):
+    """n uniform points in the bounding box of V."""
+    lo, hi = V.min(0), V.max(0)
+    return rng.uniform(lo, hi, (n, V.shape[1])).astype(np.float32)

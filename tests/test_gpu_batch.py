@@ -84,3 +84,62 @@ def test_batch_forward_only(cuda):
         assert o["dV"] is None
         assert np.array_equal(_np(o["mean"]), _np(sc.solve(P, s)))
     plan.close()
+
+
+def _batched_items(n_stars, n_spheres, scale, seed=0):
+    import torch
+    from wos import BatchItem, shapes
+    from wos.native import NativeScene, WalkSettings
+    rng = np.random.default_rng(seed + 1)
+    items, exact = [], []
+    for sc in shapes.batched_scenes(seed=seed, n_stars=n_stars, n_spheres=n_spheres, scale=scale,
+                                    sphere_levels=(3, 4)):
+        ns = NativeScene(sc["V"], sc["F"], sc["g"])
+        parts, got = [], 0
+        while got < sc["n"]:
+            cand = shapes.sample_box(sc["V"], 4096, rng)
+            ins = ns.closest(cand, True, want=("inside",))["inside"].bool()
+            parts.append(torch.as_tensor(cand, device="cuda")[ins])
+            got += int(ins.sum())
+        P = torch.cat(parts)[:sc["n"]].contiguous()
+        ex = shapes.harmonic_poly(P.cpu().numpy(), sc["coeffs"], sc["degree"])
+        s = WalkSettings(nwalks=sc["nwalks"], nsteps=128, epsilon=1e-3, seed=sc["seed"])
+        items.append(BatchItem(ns, P, s, 2, torch.as_tensor(ex.astype(np.float32), device="cuda")))
+        exact.append(ex)
+    return items, exact
+
+
+def test_batched_harmonic_scenes_match_exact_solution(cuda):
+    """Seeded many-scene workload: every scene's field RMSE against the
+    exact harmonic polynomial is at the Monte Carlo standard error."""
+    from wos import BatchPlan
+    from wos.native import AdjointSettings
+    items, exact = _batched_items(6, 4, 0.02)
+    plan = BatchPlan(items, AdjointSettings(epsilon2=1e-3, clamping=0.1, want_dV=True, want_dg=True))
+    plan.run(use_graph=True)
+    for i, it in enumerate(items):
+        o = plan.outputs(i)
+        m, v = _np(o["mean"]), _np(o["var"])
+        rmse = np.sqrt(((m - exact[i]) ** 2).mean())
+        rse = np.sqrt((v / it.settings.nwalks).mean())
+        assert rmse < 1.2 * rse + 5e-3, (i, rmse, rse)
+        assert np.isfinite(_np(o["dV"])).all() and np.isfinite(_np(o["dg"])).all()
+    plan.close()
+
+
+def test_autotuned_launch_shape_does_not_change_results(cuda):
+    """Walks are defined by their Philox counters, so the launch shape the
+    tuner picks changes speed only: means are bit-identical."""
+    from wos import BatchPlan, autotune
+    items, _ = _batched_items(3, 2, 0.01, seed=7)
+    plan = BatchPlan(items, None)
+    plan.run(use_graph=False)
+    ref = [_np(plan.outputs(i)["mean"]) for i in range(len(items))]
+    best, times = autotune.tune_batch(plan, candidates=[(128, 16), (512, 64)], repeats=1)
+    assert best in times and len(times) == 2
+    for bt, chunk in ((128, 16), (512, 64), best):
+        plan.set_launch(bt, 0, chunk)
+        plan.run(use_graph=True)
+        for i in range(len(items)):
+            assert np.array_equal(_np(plan.outputs(i)["mean"]), ref[i]), (bt, chunk, i)
+    plan.close()

@@ -128,3 +128,37 @@ def test_statistics():
     st = Statistics()
     assert np.isclose(st.mean(x)[-1], x.mean())
     assert np.isclose(st.var(x)[-1], x.var())
+
+
+@pytest.mark.parametrize("dim,degree", [(2, 1), (2, 3), (3, 1), (3, 2), (3, 3)])
+def test_harmonic_basis_is_harmonic(dim, degree):
+    from wos import shapes
+    rng = np.random.default_rng(dim * 10 + degree)
+    P = rng.uniform(-1, 1, (64, dim))
+    h = 1e-3
+    lap = -2 * dim * shapes.harmonic_basis(P, degree)
+    for k in range(dim):
+        e = np.zeros(dim)
+        e[k] = h
+        lap = lap + shapes.harmonic_basis(P + e, degree) + shapes.harmonic_basis(P - e, degree)
+    assert np.abs(lap / h ** 2).max() < 1e-5
+    ncols = shapes.harmonic_basis(P, degree).shape[1]
+    assert ncols == (2 * degree if dim == 2 else {1: 3, 2: 8, 3: 15}[degree])
+
+
+def test_batched_scenes_ranges_and_seeding():
+    from wos import shapes
+    a = shapes.batched_scenes(seed=5, n_stars=6, n_spheres=3, scale=0.1, sphere_levels=(2, 3))
+    b = shapes.batched_scenes(seed=5, n_stars=6, n_spheres=3, scale=0.1, sphere_levels=(2, 3))
+    assert len(a) == 9
+    for x, y in zip(a, b):
+        assert np.array_equal(x["V"], y["V"]) and np.array_equal(x["g"], y["g"]) and x["seed"] == y["seed"]
+    for sc in a:
+        assert 16 <= sc["nwalks"] <= 256 and 1 <= sc["degree"] <= 3
+        assert 100 <= sc["n"] <= 20000
+        if sc["dim"] == 2:
+            assert 256 <= sc["F"].shape[0] <= 16384
+        else:
+            assert sc["F"].shape[0] in (320, 1280)
+        np.testing.assert_allclose(sc["g"], shapes.harmonic_poly(sc["V"], sc["coeffs"], sc["degree"]), rtol=1e-5,
+                                   atol=1e-5)
