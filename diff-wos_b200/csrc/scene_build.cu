@@ -360,25 +360,93 @@ __global__ void k_leaf_data(const unsigned long long *keys, int n, const float4 
     }
 }
 
-// Wide-tree boxes.  Level 1 node i bounds Morton positions [32 i, 32 i + 32).
+// Wide-tree leaves.  Leaf i holds Morton positions [WT_LEAF i, WT_LEAF i +
+// WT_LEAF): its box, and its slab bound -- n = the normalised sum of the
+// primitives' unit normals, c = the box centre computed exactly as the query
+// does, and [oc - oh, oc + oh] covering n.(v - c) over the primitives'
+// vertices as the distance code sees them (a and a + d for a segment, a,
+// a + ab, a + ac for a triangle), evaluated in double and widened by the
+// float roundings plus a relative margin.  A leaf whose normals cancel gets
+// n = 0 and oh = inf (no slab bound).
 template <int D>
-__global__ void k_wt_level1(const unsigned long long *keys, int nF, const float *pbox, float4 *out, int n1) {
+__global__ void k_wt_level1(const unsigned long long *keys, int nF, const float *pbox, const float4 *lseg,
+                            const float4 *ltri, float4 *out, float4 *slab, int n1) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n1) return;
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    const int e = min(32 * i + 32, nF);
-    for (int s = 32 * i; s < e; ++s) {
+    const int b0 = WT_LEAF * i, e = min(b0 + WT_LEAF, nF);
+    double ns[3] = {0.0, 0.0, 0.0};
+    for (int s = b0; s < e; ++s) {
         const float *b = pbox + (size_t)(unsigned)keys[s] * 2 * D;
         for (int k = 0; k < D; ++k) {
             lo[k] = fminf(lo[k], b[k]);
             hi[k] = fmaxf(hi[k], b[D + k]);
         }
+        double nn[3] = {0.0, 0.0, 0.0};
+        if (D == 2) {
+            const float4 g = lseg[s];
+            nn[0] = (double)g.w;
+            nn[1] = -(double)g.z;
+        } else {
+            const float4 ab = ltri[3 * s + 1], ac = ltri[3 * s + 2];
+            nn[0] = (double)ab.y * ac.z - (double)ab.z * ac.y;
+            nn[1] = (double)ab.z * ac.x - (double)ab.x * ac.z;
+            nn[2] = (double)ab.x * ac.y - (double)ab.y * ac.x;
+        }
+        const double l = sqrt(nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2]);
+        if (l > 0.0)
+            for (int k = 0; k < 3; ++k) ns[k] += nn[k] / l;
+    }
+    float c[3] = {0.0f, 0.0f, 0.0f};
+    for (int k = 0; k < D; ++k) c[k] = (lo[k] + hi[k]) * 0.5f;
+    const double ln = sqrt(ns[0] * ns[0] + ns[1] * ns[1] + ns[2] * ns[2]);
+    float nf[3] = {0.0f, 0.0f, 0.0f};
+    float ocf = 0.0f, ohf = INFINITY;
+    if (ln > 1e-6) {
+        // unit normal, shrunk by 2^-20 so that |n| <= 1 after rounding
+        for (int k = 0; k < D; ++k) nf[k] = (float)(ns[k] / ln * (1.0 - 0x1p-20));
+        double omin = INFINITY, omax = -INFINITY, diag2 = 0.0;
+        for (int k = 0; k < D; ++k) diag2 += ((double)hi[k] - lo[k]) * ((double)hi[k] - lo[k]);
+        for (int s = b0; s < e; ++s) {
+            double v[3][3];
+            int nv;
+            if (D == 2) {
+                const float4 g = lseg[s];
+                v[0][0] = g.x;
+                v[0][1] = g.y;
+                v[1][0] = (double)g.x + g.z;
+                v[1][1] = (double)g.y + g.w;
+                v[0][2] = v[1][2] = 0.0;
+                nv = 2;
+            } else {
+                const float4 a = ltri[3 * s], ab = ltri[3 * s + 1], ac = ltri[3 * s + 2];
+                const double av[3] = {a.x, a.y, a.z}, abv[3] = {ab.x, ab.y, ab.z}, acv[3] = {ac.x, ac.y, ac.z};
+                for (int k = 0; k < 3; ++k) {
+                    v[0][k] = av[k];
+                    v[1][k] = av[k] + abv[k];
+                    v[2][k] = av[k] + acv[k];
+                }
+                nv = 3;
+            }
+            for (int j = 0; j < nv; ++j) {
+                double o = 0.0;
+                for (int k = 0; k < D; ++k) o += (double)nf[k] * (v[j][k] - (double)c[k]);
+                omin = fmin(omin, o);
+                omax = fmax(omax, o);
+            }
+        }
+        const double oc = 0.5 * (omin + omax);
+        ocf = (float)oc;
+        const double oh = 0.5 * (omax - omin) + fabs(oc - (double)ocf) + 1e-6 * sqrt(diag2);
+        ohf = __double2float_ru(oh);
     }
     if (D == 2) {
         out[i] = make_float4(lo[0], lo[1], hi[0], hi[1]);
+        slab[i] = make_float4(nf[0], nf[1], ocf, ohf);
     } else {
-        out[2 * i] = make_float4(lo[0], lo[1], lo[2], 0.0f);
+        out[2 * i] = make_float4(lo[0], lo[1], lo[2], ohf);
         out[2 * i + 1] = make_float4(hi[0], hi[1], hi[2], 0.0f);
+        slab[i] = make_float4(nf[0], nf[1], nf[2], ocf);
     }
 }
 
@@ -423,7 +491,7 @@ static cudaError_t dalloc(T **p, size_t count, cudaStream_t st) {
 }
 
 void SceneImpl::release(cudaStream_t st) {
-    void *ptrs[] = {V, F, N, g, seg, seginv, tri, node, lseg, lseginv, ltri, lorig, cdf, wt_box, guide};
+    void *ptrs[] = {V, F, N, g, seg, seginv, tri, node, lseg, lseginv, ltri, lorig, cdf, wt_box, wt_slab, guide};
     for (void *p : ptrs)
         if (p) cudaFreeAsync(p, st);
     V = nullptr;
@@ -440,6 +508,7 @@ void SceneImpl::release(cudaStream_t st) {
     lorig = nullptr;
     cdf = nullptr;
     wt_box = nullptr;
+    wt_slab = nullptr;
     guide = nullptr;
 }
 
@@ -556,7 +625,7 @@ static int build_geometry(SceneImpl &S, cudaStream_t st) {
     // ---- wide tree (levels 1..wt_levels, the top one with <= 32 nodes)
     {
         const int W = D == 2 ? 1 : 2;  // float4 per box
-        int count = (nF + 31) / 32, level = 1, off = 0;
+        int count = (nF + WT_LEAF - 1) / WT_LEAF, level = 1, off = 0;
         S.wt_count[0] = nF;
         for (;;) {
             if (level > WT_MAX_LEVELS) return fail(WOS_ERR_UNSUPPORTED, "scene too large for the wide tree");
@@ -571,7 +640,11 @@ static int build_geometry(SceneImpl &S, cudaStream_t st) {
         if (S.wt_box) cudaFreeAsync(S.wt_box, st);
         S.wt_box = nullptr;
         WOS_TRY(dalloc(&S.wt_box, (size_t)off * W, st));
-        k_wt_level1<D><<<nblk(S.wt_count[1], TB), TB, 0, st>>>(skeys, nF, pbox, S.wt_box, S.wt_count[1]);
+        if (S.wt_slab) cudaFreeAsync(S.wt_slab, st);
+        S.wt_slab = nullptr;
+        WOS_TRY(dalloc(&S.wt_slab, (size_t)S.wt_count[1], st));
+        k_wt_level1<D><<<nblk(S.wt_count[1], TB), TB, 0, st>>>(skeys, nF, pbox, S.lseg, S.ltri, S.wt_box, S.wt_slab,
+                                                               S.wt_count[1]);
         for (int l = 2; l <= S.wt_levels; ++l)
             k_wt_level<D><<<nblk(S.wt_count[l], TB), TB, 0, st>>>(S.wt_box + (size_t)S.wt_off[l - 1] * W,
                                                                 S.wt_count[l - 1], S.wt_box + (size_t)S.wt_off[l] * W,
@@ -718,6 +791,7 @@ SceneView SceneImpl::view() const {
         v.wt_off[k] = wt_off[k];
     }
     v.wt_box = wt_box;
+    v.wt_slab = wt_slab;
     return v;
 }
 

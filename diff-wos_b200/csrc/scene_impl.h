@@ -50,6 +50,7 @@ struct SceneImpl {
     int wt_count[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int wt_off[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     float4 *wt_box = nullptr;
+    float4 *wt_slab = nullptr;
 
     int allocate(cudaStream_t st);
     int check_indices(cudaStream_t st);

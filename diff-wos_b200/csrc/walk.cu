@@ -75,9 +75,13 @@ __device__ __forceinline__ void flush_work(const Work &wk) {
 // Nearest query of every active lane.  With the LBVH the lanes take turns:
 // the whole warp answers each lane's query cooperatively (wquery), starting
 // from the warm candidate `warm` (that lane's previous nearest primitive, or
-// -1).  Brute force runs per lane.  Must be called by all 32 lanes.
+// -1).  A lane with ball_m > 0 asks instead for a primitive blocking the
+// ball of radius ball_m centred at x (wball): it gets that primitive, or
+// prim = -1 when none blocks.  Brute force runs per lane and always returns
+// the nearest primitive.  Must be called by all 32 lanes.
 template <int D, bool BVH>
-__device__ __forceinline__ Hit warp_queries(const SceneView &S, bool active, const float *x, int warm, Work &work) {
+__device__ __forceinline__ Hit warp_queries(const SceneView &S, bool active, const float *x, int warm, Work &work,
+                                            float ball_m = -1.0f) {
     Hit mine{-1, INFINITY};
     if (!BVH) {
         if (active) mine = nearest_brute<D>(S, x, work);
@@ -94,12 +98,17 @@ __device__ __forceinline__ Hit warp_queries(const SceneView &S, bool active, con
         q[1] = __shfl_sync(FULL, x[1], j);
         q[2] = D == 3 ? __shfl_sync(FULL, x[2], j) : 0.0f;
         const int wp = __shfl_sync(FULL, warm, j);
-        Hit best{-1, INFINITY};
-        if (wp >= 0) {
-            best.prim = wp;
-            best.d2 = prim_d2<D>(S, wp, q);
+        const float bm = __shfl_sync(FULL, ball_m, j);
+        Hit h{-1, INFINITY};
+        if (bm > 0.0f) {
+            wball<D>(S, q, bm, h, work);
+        } else {
+            if (wp >= 0) {
+                h.prim = wp;
+                h.d2 = prim_d2<D>(S, wp, q);
+            }
+            h = wquery<D>(S, q, h, work);
         }
-        const Hit h = wquery<D>(S, q, best, work);
         if (lane == j) mine = h;
     }
     return mine;
@@ -134,6 +143,8 @@ template <int D>
 __device__ __forceinline__ int walker_advance(Walker &w, const SceneView &S, const Hit &hit, const WalkCfg &c,
                                               float eps, bool project, bool prevent_fd, uint32_t pt, uint32_t wk,
                                               uint32_t role, bool want_ds, const unsigned short *guide) {
+    // no primitive at a finite distance (a NaN or overflowing point)
+    if (hit.prim < 0) return W_INVALID;
     float d = sqrtf(hit.d2);
     if (w.fresh) {
         w.fresh = false;
@@ -216,7 +227,6 @@ __device__ __forceinline__ bool refill(Queue &q, bool &active, long long &idx, u
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     unsigned idle = __ballot_sync(FULL, !active);
-    bool got = false;
     while (idle != 0u && !q.drained) {
         if (q.cb >= q.ce) {
             unsigned long long base = 0;
@@ -235,12 +245,10 @@ __device__ __forceinline__ bool refill(Queue &q, bool &active, long long &idx, u
         if (!active && rank < avail) {
             idx = q.cb + rank;
             active = true;
-            got = true;
         }
         q.cb += avail;
         idle = __ballot_sync(FULL, !active);
     }
-    (void)got;
     return __ballot_sync(FULL, active) != 0u;
 }
 
@@ -437,7 +445,7 @@ __device__ __forceinline__ float inscribed_ball(const SceneView &S, const float 
 #pragma unroll
         for (int k = 0; k < D; ++k) q[k] = fmaf(n[k], m, p[k]);
         const float d = sqrtf(query<D, BVH>(S, q, top, n_top, work).d2);
-        if (fabsf(d - m) < 1e-5f)
+        if (wosm::ball_accepts(d, m))
             a = m;
         else
             b = m;
@@ -600,6 +608,31 @@ __device__ __forceinline__ void nd_finish(const NdState &st, const SceneView &S,
     for (int k = 0; k < D; ++k) out[k] = grad * st.n[k];
 }
 
+// Lane-local part of one inscribed-ball bisection step at radius m, centre q:
+// the primitive that blocked the previous rejected radius decides a
+// rejection without a query (need = false, pre = that primitive); otherwise,
+// if the ball's own primitive rprim is within m + 1e-5f, the step is accepted
+// unless some primitive blocks, and the warp only searches for one
+// (ball_m = m; pre = rprim, the result when none blocks).  Else the step
+// takes the full nearest query (the reference's test on the nearest distance).
+template <int D>
+__device__ __forceinline__ void ball_precheck(const SceneView &S, const float *q, float m, int bwarm, int rprim,
+                                              bool &need, float &ball_m, Hit &pre) {
+    if (bwarm >= 0) {
+        const float d2 = prim_d2<D>(S, bwarm, q);
+        if (ball_blocks(d2, m)) {
+            pre = Hit{bwarm, d2};
+            need = false;
+            return;
+        }
+    }
+    const float d2 = prim_d2<D>(S, rprim, q);
+    if (sqrtf(d2) - m <= 1e-5f) {
+        pre = Hit{rprim, d2};
+        ball_m = m;
+    }
+}
+
 enum { PH_IDLE = 0, PH_PRIMAL = 1, PH_BALL = 2, PH_ANTI_START = 3, PH_ANTI_WALK = 4, PH_ND_START = 5 };
 
 // Per-thread adjoint state kept in shared memory: touched at phase changes,
@@ -610,14 +643,17 @@ struct AdjSlot {
     float rt0, rt1;
     float ba, bb;  // bisection bracket
     int bk;
+    int bwarm;     // primitive that blocked the last rejected radius, or -1
     double acc[5];  // source-parameter gradient accumulators
 };
 constexpr int ADJ_THREAD_WORDS = (int)((sizeof(AdjSlot) + 7) / 8);
 
 // The adjoint kernel runs at most 256 threads per block and is compiled for
-// at least ADJ_MIN_BLOCKS resident blocks per SM (a register cap).
+// at least ADJ_MIN_BLOCKS resident blocks per SM: a 64-register cap.  The 3D
+// kernel spills a little at that cap and is still faster than at 80
+// registers and three blocks.
 #ifndef ADJ_MIN_BLOCKS
-#define ADJ_MIN_BLOCKS 3
+#define ADJ_MIN_BLOCKS 4
 #endif
 
 // Persistent adjoint kernel.  ND_ONLY: the items are boundary records and the
@@ -641,6 +677,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
     float &rt0 = slot.rt0, &rt1 = slot.rt1;
     float &ba = slot.ba, &bb = slot.bb;
     int &bk = slot.bk;
+    int &bwarm = slot.bwarm;
     const bool src2 = D == 2 && S.src_type != 0;
     constexpr bool ND_ONLY = MODE == ADJ_ND_ONLY;
     const bool want_src = !ND_ONLY && a.want_dsrc && c.include_source && src2;
@@ -731,6 +768,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
                             ba = a.ball_eps;
                             bb = S.half_min_extent;
                             bk = 0;
+                            bwarm = -1;
                             const float m = (ba + bb) * 0.5f;
 #pragma unroll
                             for (int k = 0; k < D; ++k) qpos[k] = fmaf(rn[k], m, st.p[k]);
@@ -746,6 +784,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
             ba = a.ball_eps;
             bb = S.half_min_extent;
             bk = 0;
+            bwarm = -1;
             const float m = (ba + bb) * 0.5f;
 #pragma unroll
             for (int k = 0; k < D; ++k) qpos[k] = fmaf(rn[k], m, st.p[k]);
@@ -755,8 +794,13 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
         float x[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) x[k] = walking ? w.p[k] : qpos[k];
-        const Hit hit = warp_queries<D, BVH>(S, active, x, walking ? w.last : rprim, work);
+        bool need = active;
+        float ball_m = -1.0f;
+        Hit pre{-1, INFINITY};
+        if (active && phase == PH_BALL) ball_precheck<D>(S, qpos, (ba + bb) * 0.5f, bwarm, rprim, need, ball_m, pre);
+        Hit hit = warp_queries<D, BVH>(S, need, x, walking ? w.last : rprim, work, ball_m);
         if (!active) continue;
+        if (phase == PH_BALL && (!need || (ball_m > 0.0f && hit.prim < 0))) hit = pre;
         if (walking) w.last = hit.prim;
         bool finish_anti = false;
         float uq = 0.0f;
@@ -795,6 +839,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
             ba = a.ball_eps;
             bb = S.half_min_extent;
             bk = 0;
+            bwarm = -1;
             const float m = (ba + bb) * 0.5f;
 #pragma unroll
             for (int k = 0; k < D; ++k) qpos[k] = fmaf(rn[k], m, st.p[k]);
@@ -804,10 +849,12 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
         if (phase == PH_BALL) {
             const float d = sqrtf(hit.d2);
             const float m = (ba + bb) * 0.5f;
-            if (fabsf(d - m) < 1e-5f)
+            if (wosm::ball_accepts(d, m)) {
                 ba = m;
-            else
+            } else {
                 bb = m;
+                bwarm = hit.prim;
+            }
             ++bk;
             if (bk < 10) {
                 const float m2 = (ba + bb) * 0.5f;
@@ -1225,7 +1272,7 @@ __device__ __forceinline__ int find_item_point(const BatchItemDev *__restrict__ 
 
 template <int D>
 __device__ __forceinline__ Hit warp_queries_batch(const SceneView *__restrict__ views, bool active, int item,
-                                                  const float *x, int warm, Work &work) {
+                                                  const float *x, int warm, Work &work, float ball_m = -1.0f) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     Hit mine{-1, INFINITY};
@@ -1239,13 +1286,18 @@ __device__ __forceinline__ Hit warp_queries_batch(const SceneView *__restrict__ 
         q[2] = D == 3 ? __shfl_sync(FULL, x[2], j) : 0.0f;
         const int wp = __shfl_sync(FULL, warm, j);
         const int it = __shfl_sync(FULL, item, j);
+        const float bm = __shfl_sync(FULL, ball_m, j);
         const SceneView &Sj = views[it];
-        Hit best{-1, INFINITY};
-        if (wp >= 0) {
-            best.prim = wp;
-            best.d2 = prim_d2<D>(Sj, wp, q);
+        Hit h{-1, INFINITY};
+        if (bm > 0.0f) {
+            wball<D>(Sj, q, bm, h, work);
+        } else {
+            if (wp >= 0) {
+                h.prim = wp;
+                h.d2 = prim_d2<D>(Sj, wp, q);
+            }
+            h = wquery<D>(Sj, q, h, work);
         }
-        const Hit h = wquery<D>(Sj, q, best, work);
         if (lane == j) mine = h;
     }
     return mine;
@@ -1385,6 +1437,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
     float &rt0 = slot.rt0, &rt1 = slot.rt1;
     float &ba = slot.ba, &bb = slot.bb;
     int &bk = slot.bk;
+    int &bwarm = slot.bwarm;
     Queue q{0, 0, false};
     bool active = false;
     long long idx = 0;
@@ -1459,6 +1512,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
                     ba = a.ball_eps;
                     bb = S.half_min_extent;
                     bk = 0;
+                    bwarm = -1;
                     const float m = (ba + bb) * 0.5f;
 #pragma unroll
                     for (int k = 0; k < D; ++k) qpos[k] = fmaf(rn[k], m, st.p[k]);
@@ -1469,8 +1523,14 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
         float x[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) x[k] = walking ? w.p[k] : qpos[k];
-        const Hit hit = warp_queries_batch<D>(views, active, item, x, walking ? w.last : rprim, work);
+        bool need = active;
+        float ball_m = -1.0f;
+        Hit pre{-1, INFINITY};
+        if (active && phase == PH_BALL)
+            ball_precheck<D>(views[item], qpos, (ba + bb) * 0.5f, bwarm, rprim, need, ball_m, pre);
+        Hit hit = warp_queries_batch<D>(views, need, item, x, walking ? w.last : rprim, work, ball_m);
         if (!active) continue;
+        if (phase == PH_BALL && (!need || (ball_m > 0.0f && hit.prim < 0))) hit = pre;
         const SceneView &S = views[item];
         const WalkCfg &c = cfgs[item];
         const bool with_src = a.source_in_nd && D == 2 && S.src_type != 0;
@@ -1480,10 +1540,12 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
         if (phase == PH_BALL) {
             const float d = sqrtf(hit.d2);
             const float m = (ba + bb) * 0.5f;
-            if (fabsf(d - m) < 1e-5f)
+            if (wosm::ball_accepts(d, m)) {
                 ba = m;
-            else
+            } else {
                 bb = m;
+                bwarm = hit.prim;
+            }
             ++bk;
             if (bk < 10) {
                 const float m2 = (ba + bb) * 0.5f;

@@ -7,6 +7,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <float.h>
 #include <stdint.h>
 
 #include "wos_math.h"
@@ -60,19 +61,31 @@ struct SceneView {
     // brackets the CDF search to a few entries
     const unsigned short *guide;
     int n_guide;
-    // Wide tree for the warp-cooperative query: an implicit 32-ary tree over
-    // the Morton-ordered primitives.  Level 1 node i bounds primitives
-    // [32 i, 32 i + 32) (in Morton order), level k node i bounds level k-1
-    // nodes [32 i, 32 i + 32); level wt_levels has at most 32 nodes.  Boxes:
-    // 2D one float4 (lo.x, lo.y, hi.x, hi.y) per node, 3D two float4
-    // (lo.xyz, 0), (hi.xyz, 0); level k starts at wt_box[wt_off[k]] (in nodes).
+    // Wide tree for the warp-cooperative query: an implicit tree over the
+    // Morton-ordered primitives.  Level 1 nodes are leaves, leaf i holding
+    // primitives [WT_LEAF i, WT_LEAF i + WT_LEAF) (in Morton order); level k
+    // node i bounds level k-1 nodes [32 i, 32 i + 32); level wt_levels has at
+    // most 32 nodes.  Boxes: 2D one float4 (lo.x, lo.y, hi.x, hi.y) per node,
+    // 3D two float4 (lo.xyz, w), (hi.xyz, 0) with w = 0 except at leaves; level
+    // k starts at wt_box[wt_off[k]] (in nodes).  Each leaf also has a slab
+    // bound: unit normal n and [oc - oh, oc + oh] containing n.(v - c) for
+    // every vertex v of its primitives, c the box centre; 2D wt_slab[i] =
+    // (n.x, n.y, oc, oh), 3D wt_slab[i] = (n.xyz, oc) with oh in the leaf
+    // box's lo.w.  Any point y of the leaf is at least |n.(x - c) - oc| - oh
+    // from x, which for flat patches tilted against the axes is far tighter
+    // than the box.
     int wt_levels;
     int wt_count[8];
     int wt_off[8];
     const float4 *wt_box;
+    const float4 *wt_slab;
 };
 
 constexpr int WT_MAX_LEVELS = 5;
+// Primitives per leaf: one per lane.  (Leaves of 8 or 16 primitives, four or
+// two tested per warp step, were measured slower on both the 2D and the 3D
+// workloads: the extra pops cost more than the tighter leaves save.)
+constexpr int WT_LEAF = 32;
 
 template <int D>
 struct NodeWords;
@@ -195,6 +208,71 @@ __device__ __forceinline__ float tri_closest(float4 t0, float4 t1, float4 t2, fl
     dx = fmaf(-t2.x, w, fmaf(-t1.x, v, axx));
     dy = fmaf(-t2.y, w, fmaf(-t1.y, v, axy));
     dz = fmaf(-t2.z, w, fmaf(-t1.z, v, axz));
+    return dot3(dx, dy, dz, dx, dy, dz);
+}
+
+// Squared distance to a triangle for warp-wide leaf tests: a branch-free
+// form of tri_closest's region cascade.  Every region test is evaluated with
+// the cascade's own expressions, the first region that holds
+// picks the result, and the one division the edge and face regions need is
+// issued once with the selected numerator and denominator.  Each value is the
+// same IEEE operation on the same operands as in the cascade, so the results
+// are identical to tri_closest's, but the lanes of a warp testing different
+// triangles do not diverge (and run one division instead of up to four in
+// turn).  Per-thread searches keep the cascade, which skips work per lane.
+__device__ __forceinline__ float tri_d2_uniform(float4 t0, float4 t1, float4 t2, float x, float y, float z) {
+    const float axx = x - t0.x, axy = y - t0.y, axz = z - t0.z;
+    const float ab2 = t0.w, abac = t1.w, ac2 = t2.w;
+    const float d1 = dot3(t1.x, t1.y, t1.z, axx, axy, axz);
+    const float d2 = dot3(t2.x, t2.y, t2.z, axx, axy, axz);
+    const float d3 = d1 - ab2, d4 = d2 - abac;
+    const float d5 = d1 - abac, d6 = d2 - ac2;
+    const float vc = d1 * d4 - d3 * d2;
+    const float vb = d5 * d2 - d1 * d6;
+    const float va = d3 * d6 - d5 * d4;
+    const float e43 = d4 - d3, e56 = d5 - d6;
+    const float sum = va + vb + vc;
+    const bool rA = d1 <= 0.0f && d2 <= 0.0f;                  // vertex a
+    const bool rB = d3 >= 0.0f && d4 <= d3;                    // vertex b
+    const bool rC = d6 >= 0.0f && d5 <= d6;                    // vertex c
+    const bool rAB = vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f;   // edge ab
+    const bool rAC = vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f;   // edge ac
+    const bool rBC = va <= 0.0f && e43 >= 0.0f && e56 >= 0.0f; // edge bc
+    // numerator / denominator of the first edge region that holds, else the face
+    float num = 1.0f, den = sum;
+    if (rBC) {
+        num = e43;
+        den = e43 + e56;
+    }
+    if (rAC) {
+        num = d2;
+        den = d2 - d6;
+    }
+    if (rAB) {
+        num = d1;
+        den = d1 - d3;
+    }
+    const float q = num / den;
+    float v = 0.0f, w = 0.0f;
+    if (rA) {
+    } else if (rB) {
+        v = 1.0f;
+    } else if (rC) {
+        w = 1.0f;
+    } else if (rAB) {
+        v = q;
+    } else if (rAC) {
+        w = q;
+    } else if (rBC) {
+        w = q;
+        v = 1.0f - q;
+    } else if (sum > 0.0f) {
+        v = vb * q;
+        w = vc * q;
+    }
+    const float dx = fmaf(-t2.x, w, fmaf(-t1.x, v, axx));
+    const float dy = fmaf(-t2.y, w, fmaf(-t1.y, v, axy));
+    const float dz = fmaf(-t2.z, w, fmaf(-t1.z, v, axz));
     return dot3(dx, dy, dz, dx, dy, dz);
 }
 
@@ -425,6 +503,38 @@ __device__ __forceinline__ float wt_box_d2(const SceneView &S, int node, const f
     return box_d2<D>(lo, hi, q);
 }
 
+// Lower bound on the squared distance from q to leaf `leaf`: in 3D the
+// larger of its box distance and its slab distance; in 2D the box distance
+// (polyline pieces are thin enough in their boxes that the slab test costs
+// more than it prunes).
+template <int D>
+__device__ __forceinline__ float leaf_bound(const SceneView &S, int leaf, const float *q) {
+    float lo[3], hi[3], n[3], c[3], oc, oh;
+    if (D == 2) {
+        return wt_box_d2<2>(S, S.wt_off[1] + leaf, q);
+    } else {
+        const float4 a = __ldg(&S.wt_box[2 * (S.wt_off[1] + leaf)]), b = __ldg(&S.wt_box[2 * (S.wt_off[1] + leaf) + 1]);
+        const float4 sl = __ldg(&S.wt_slab[leaf]);
+        lo[0] = a.x;
+        lo[1] = a.y;
+        lo[2] = a.z;
+        hi[0] = b.x;
+        hi[1] = b.y;
+        hi[2] = b.z;
+        n[0] = sl.x;
+        n[1] = sl.y;
+        n[2] = sl.z;
+        oc = sl.w;
+        oh = a.w;
+    }
+    const float bd = box_d2<D>(lo, hi, q);
+#pragma unroll
+    for (int k = 0; k < D; ++k) c[k] = (lo[k] + hi[k]) * 0.5f;
+    const float t = dot3(n[0], n[1], n[2], q[0] - c[0], q[1] - c[1], q[2] - c[2]);
+    const float lb = fabsf(t - oc) - oh;
+    return lb > 0.0f ? fmaxf(bd, lb * lb) : bd;
+}
+
 // Squared distance to the primitive at Morton position s.
 template <int D>
 __device__ __forceinline__ float leaf_d2(const SceneView &S, int s, const float *q) {
@@ -432,7 +542,8 @@ __device__ __forceinline__ float leaf_d2(const SceneView &S, int s, const float 
         float t;
         return seg_d2(__ldg(&S.lseg[s]), __ldg(&S.lseginv[s]), q[0], q[1], t);
     }
-    return tri_d2(__ldg(&S.ltri[3 * s]), __ldg(&S.ltri[3 * s + 1]), __ldg(&S.ltri[3 * s + 2]), q[0], q[1], q[2]);
+    return tri_d2_uniform(__ldg(&S.ltri[3 * s]), __ldg(&S.ltri[3 * s + 1]), __ldg(&S.ltri[3 * s + 2]), q[0], q[1],
+                          q[2]);
 }
 
 // Squared distance to primitive f in the original order.
@@ -445,14 +556,20 @@ __device__ __forceinline__ float prim_d2(const SceneView &S, int f, const float 
     return tri_d2(__ldg(&S.tri[3 * f]), __ldg(&S.tri[3 * f + 1]), __ldg(&S.tri[3 * f + 2]), q[0], q[1], q[2]);
 }
 
+// Pruning bound of the wide-tree descent, clamped to the largest float so
+// that +inf frontier entries (no child) are never taken, even before a first
+// candidate exists or when the query point is NaN or overflows.
+__device__ __forceinline__ float wt_bound(float best, float tol2) { return fminf(prune_bound(best, tol2), FLT_MAX); }
+
 // Warp-cooperative nearest primitive for one query point q (the same q in
 // every lane; every lane returns the same Hit).  Best-first descent of the
 // wide tree, one template instance per level: the level's frontier of up to
 // 32 child distances is one register per lane, the nearest unexpanded child
 // is a redux.sync minimum, and a node expansion is one coalesced load of 32
-// boxes or 32 primitives.  `best` may hold a warm-start candidate (a real
-// primitive with its distance); pruning is conservative, so the result is the
-// exact minimum of (d2, primitive index) -- the same as the brute-force search.
+// boxes (leaf bounds at level 1) or 32 primitives.  `best` may hold a
+// warm-start candidate (a real primitive with its distance); pruning is
+// conservative, so the result is the exact minimum of (d2, primitive index)
+// -- the same as the brute-force search.
 template <int D, int L>
 __device__ __forceinline__ void wdescend(const SceneView &S, const float *q, int first, float tol2, Hit &best,
                                          Work &wk) {
@@ -460,21 +577,21 @@ __device__ __forceinline__ void wdescend(const SceneView &S, const float *q, int
     const int lane = threadIdx.x & 31;
     const int child = first + lane;
     float d = INFINITY;
-    if (child < S.wt_count[L]) d = wt_box_d2<D>(S, S.wt_off[L] + child, q);
+    if (child < S.wt_count[L]) d = L == 1 ? leaf_bound<D>(S, child, q) : wt_box_d2<D>(S, S.wt_off[L] + child, q);
     wk.nb += 1;
     for (;;) {
         const float m = warp_min(d);
-        if (m > prune_bound(best.d2, tol2)) return;
+        if (m > wt_bound(best.d2, tol2)) return;
         const int j = __ffs(__ballot_sync(FULL, d == m)) - 1;
         if (lane == j) d = INFINITY;
         const int node = first + j;
         if constexpr (L == 1) {
             wk.np += 1;
-            const int s = node * 32 + lane;
+            const int s = node * WT_LEAF + lane;
             float d2 = INFINITY;
             if (s < S.nF) d2 = leaf_d2<D>(S, s, q);
             const float m2 = warp_min(d2);
-            if (m2 <= best.d2) {
+            if (m2 <= best.d2 && m2 < INFINITY) {
                 const unsigned c2 = __ballot_sync(FULL, d2 == m2);
                 int o = 0x7fffffff;
                 if ((c2 >> lane) & 1u) o = __ldg(&S.lorig[s]);
@@ -502,6 +619,69 @@ __device__ __forceinline__ Hit wquery(const SceneView &S, const float *q, Hit be
         default: wdescend<D, 5>(S, q, 0, tol2, best, wk); break;
     }
     return best;
+}
+
+// ------------------------------------------------------------------ ball test
+// One bisection step of the inscribed-ball search accepts the radius m when
+// |d - m| <= 1e-5f for the nearest distance d from the candidate centre
+// (wosm::ball_accepts).  Since fl(sqrtf(d2) - m) is non-decreasing in d2, the
+// step rejects exactly when some primitive "blocks" the ball,
+// sqrtf(d2) - m < -1e-5f, or when even the nearest distance is above
+// m + 1e-5f; the caller rules the second case out with the ball's own
+// primitive.  So a step needs no nearest search: it stops at the first
+// blocking primitive.
+__device__ __forceinline__ bool ball_blocks(float d2, float m) { return sqrtf(d2) - m < -1e-5f; }
+
+template <int D, int L>
+__device__ __forceinline__ bool wball_descend(const SceneView &S, const float *q, int first, float bound, float m,
+                                              Hit &hit, Work &wk) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int child = first + lane;
+    float d = INFINITY;
+    if (child < S.wt_count[L]) d = L == 1 ? leaf_bound<D>(S, child, q) : wt_box_d2<D>(S, S.wt_off[L] + child, q);
+    wk.nb += 1;
+    for (;;) {
+        const float mn = warp_min(d);
+        if (mn > bound) return false;
+        const int j = __ffs(__ballot_sync(FULL, d == mn)) - 1;
+        if (lane == j) d = INFINITY;
+        const int node = first + j;
+        if constexpr (L == 1) {
+            wk.np += 1;
+            const int s = node * WT_LEAF + lane;
+            float d2 = INFINITY;
+            if (s < S.nF) d2 = leaf_d2<D>(S, s, q);
+            const unsigned b = __ballot_sync(FULL, s < S.nF && ball_blocks(d2, m));
+            if (b) {
+                const int src = __ffs(b) - 1;
+                int o = 0;
+                if (lane == src) o = __ldg(&S.lorig[s]);
+                hit.prim = __shfl_sync(FULL, o, src);
+                hit.d2 = __shfl_sync(FULL, d2, src);
+                return true;
+            }
+        } else {
+            if (wball_descend<D, L - 1>(S, q, node * 32, bound, m, hit, wk)) return true;
+        }
+    }
+}
+
+// Warp-cooperative blocking-primitive search for a ball of radius m centred
+// at q: returns true with a blocking primitive in `hit`, or false when no
+// primitive blocks.  Boxes are pruned against m^2 with the nearest search's
+// conservative tolerance, so no blocking primitive is missed.
+template <int D>
+__device__ __forceinline__ bool wball(const SceneView &S, const float *q, float m, Hit &hit, Work &wk) {
+    const float bound = wt_bound((m * m) * (1.0f + 0x1p-20f), prune_tol2<D>(S, q));
+    wk.nq += 1;
+    switch (S.wt_levels) {
+        case 1: return wball_descend<D, 1>(S, q, 0, bound, m, hit, wk);
+        case 2: return wball_descend<D, 2>(S, q, 0, bound, m, hit, wk);
+        case 3: return wball_descend<D, 3>(S, q, 0, bound, m, hit, wk);
+        case 4: return wball_descend<D, 4>(S, q, 0, bound, m, hit, wk);
+        default: return wball_descend<D, 5>(S, q, 0, bound, m, hit, wk);
+    }
 }
 
 // ------------------------------------------------------------------ records

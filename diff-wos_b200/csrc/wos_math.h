@@ -42,6 +42,12 @@ static constexpr float kPiO4   = (float)0.78539816339744830962;
 
 WOS_HD float fabs_(float x) { return fabsf(x); }
 
+// Acceptance test of one bisection step of the largest inscribed ball
+// (include/scene.cuh:233-234).  The reference compares the float |d - m|
+// with the double literal 1e-5; 1e-5f lies just below 1e-5 and the next float
+// above it, so for floats that test is |d - m| <= 1e-5f.
+WOS_HD bool ball_accepts(float d, float m) { return fabsf(d - m) <= 1e-5f; }
+
 WOS_HD uint32_t f2u(float x) {
     uint32_t u;
     memcpy(&u, &x, 4);

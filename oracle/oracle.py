@@ -136,7 +136,10 @@ class OracleScene:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().orc_scene_destroy(self.h)
+            try:
+                lib().orc_scene_destroy(self.h)
+            except TypeError:  # module globals already torn down at interpreter exit
+                pass
             self.h = None
 
     def normals(self):

@@ -753,6 +753,11 @@ static Rec walk(const Scene &S, const float *p0, const Params &prm, float eps, c
     float contrib = 0.0f, dsrc[5] = {0, 0, 0, 0, 0};
     const bool has_src = S.src_type != 0;
     for (int i = 0; i < prm.nsteps; ++i) {
+        // no primitive at a finite distance (a NaN or overflowing point)
+        if (hit.prim < 0) {
+            if (steps_out) *steps_out = i;
+            return dead;
+        }
         if (d < eps) {
             Rec r = closest_record(S, p, hit.prim);
             r.contrib = contrib;
@@ -815,7 +820,7 @@ static Rec walk(const Scene &S, const float *p0, const Params &prm, float eps, c
     }
     // the loop ran out (nsteps == 0 or projection of an unterminated walk,
     // wos/wos.py:43); without projection the walk is invalid
-    if (!prm.project_unterminated) {
+    if (!prm.project_unterminated || hit.prim < 0) {
         if (steps_out) *steps_out = prm.nsteps;
         return dead;
     }
@@ -843,7 +848,7 @@ static float inscribed_ball(const Scene &S, const Rec &r, float eps, bool bvh) {
         float q[3];
         for (int k = 0; k < S.D; ++k) q[k] = fmaf(r.n[k], m, r.p[k]);
         const float d = sqrtf(nearest(S, q, bvh).d2);
-        if (fabsf(d - m) < 1e-5f)
+        if (wosm::ball_accepts(d, m))
             a = m;
         else
             b = m;
