@@ -480,6 +480,87 @@ def c3_main(args):
     return 0
 
 
+# ---------------------------------------------------------------- inverse workload
+def inverse_run(scene, P, target, iters, nwalks, lr, dev, g0=None):
+    """Recover per-vertex Dirichlet values from interior observations: Adam
+    on g, each iteration one fused forward + adjoint of mean((u - target)^2)
+    with seed = iteration (diff-wos inv_solve loop).  Returns (g, losses)."""
+    import torch
+    from wos.native import AdjointSettings, WalkSettings
+    g = torch.zeros(scene.nV, dtype=torch.float32, device=dev) if g0 is None else g0.clone()
+    g.requires_grad_(True)
+    opt = torch.optim.Adam([g], lr=lr)
+    adj = AdjointSettings(epsilon2=1e-3, clamping=0.1, want_dV=False, want_dg=True, want_dsrc=False)
+    losses = []
+    for it in range(iters):
+        s = WalkSettings(nwalks=nwalks, nsteps=64, epsilon=1e-3, seed=it)
+        out = scene.solve_adjoint(P, s, adj, loss_kind=2, target=target)
+        losses.append(out["loss"])
+        opt.zero_grad(set_to_none=False)
+        g.grad = out["dg"]
+        opt.step()
+        with torch.no_grad():
+            scene.update_values(g.detach())
+    return g.detach(), torch.cat(losses)
+
+
+def c4_main(args):
+    """The 2D inverse problem: star r = 0.6 + 0.25 cos 5 theta with 8192
+    segments, unknown per-vertex g (initialised to 0), target = the solve with
+    g* = cos 4 theta + 0.5 sin 7 theta on the 256^2 grid masked to the
+    interior (19,988 points; 1024 walks, untimed); `--iters` Adam iterations
+    (lr 1e-2) of 32 walks per point, each a fused forward + adjoint step."""
+    import torch
+    import wos
+    from wos import shapes
+    from wos.native import NativeScene, WalkSettings
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    V, F = shapes.star(8192, 0.6, 0.25, 5)
+    th = np.arctan2(V[:, 1], V[:, 0]).astype(np.float64)
+    g_true = (np.cos(4 * th) + 0.5 * np.sin(7 * th)).astype(np.float32)
+    P = shapes.grid(256, -1.0, 1.0)
+    P = P[shapes.inside_star(P, 0.6, 0.25, 5)]
+    Pd = torch.as_tensor(np.ascontiguousarray(P), device=dev)
+    truth = NativeScene(V, F, g_true)
+    target = truth.solve(Pd, WalkSettings(nwalks=1024, nsteps=64, epsilon=1e-3, seed=12345)).to(torch.float32)
+    scene = NativeScene(V, F, np.zeros_like(g_true))
+    # warm-up iterations, then the unknowns start again from zero
+    inverse_run(scene, Pd, target, args.warmup, 32, 1e-2, dev)
+    scene.update_values(torch.zeros(len(g_true), device=dev))
+    torch.cuda.synchronize()
+    clocks = ClockSampler(None)
+    clocks.start()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    g, losses = inverse_run(scene, Pd, target, args.iters, 32, 1e-2, dev)
+    b.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t = a.elapsed_time(b) * 1e-3
+    losses = losses.cpu().numpy()
+    gt = torch.as_tensor(g_true, device=dev)
+    walks = len(P) * 32
+    line = {
+        "metric": "wos_walks_per_s", "value": walks * args.iters / t, "unit": "walks/s", "n_gpus": 1,
+        "steps": args.iters, "warmup": args.warmup, "ms_per_step": t / args.iters * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "2d_inverse_values_star8192_grid256_walks32", "points": len(P), "walks_per_point": 32,
+                   "iterations": args.iters, "optimizer": "Adam lr 1e-2", "loss": "mean((u - target)^2)",
+                   "nsteps": 64, "epsilon": 1e-3,
+                   "timed": "the whole optimisation loop: fused step, Adam update, scene value update"},
+        "iterations_per_s": args.iters / t,
+        "loss_first": float(losses[0]), "loss_last10_mean": float(losses[-10:].mean()),
+        "g_rel_error": float(torch.linalg.norm(g - gt) / torch.linalg.norm(gt)),
+        "device_status": wos.device_status(),
+    }
+    if clk is not None:
+        line["clocks"] = clk
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------- GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -492,9 +573,10 @@ def main():
     ap.add_argument("--ref-step-s", type=float, default=6.0)
     ap.add_argument("--grid", type=int, default=GRID, help="query grid (smaller only for profiling captures)")
     ap.add_argument("--walks", type=int, default=NWALKS, help="walks per point (smaller only for profiling)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "batched"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "batched"],
                     help="c2: the 2D differentiable solve (default); c3: the 3D forward + adjoint solve; "
-                         "batched: many scenes in one launch")
+                         "c4: the 2D inverse problem; batched: many scenes in one launch")
+    ap.add_argument("--iters", type=int, default=500, help="Adam iterations of the c4 workload")
     ap.add_argument("--points", type=int, default=1_000_000, help="query points of the c3 workload")
     ap.add_argument("--scale", type=float, default=0.1, help="query-count scale of the batched workload")
     args = ap.parse_args()
@@ -503,6 +585,8 @@ def main():
         return batched_main(args)
     if args.workload == "c3" and args.impl == "ours":
         return c3_main(args)
+    if args.workload == "c4" and args.impl == "ours":
+        return c4_main(args)
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
