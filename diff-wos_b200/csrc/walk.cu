@@ -137,6 +137,22 @@ struct Walker {
     }
 };
 
+// Start point of the primal walk (pt, wk): the query point, moved inside its
+// pixel when the settings carry a jitter (Detector.make_jittered_points,
+// wos/scene.py:33-39): offset (u - 1/2) * jitter per axis, u from the walk's
+// own Philox draw (role ROLE_JITTER, step 0).
+template <int D>
+__device__ __forceinline__ void walk_origin(const WalkCfg &c, const float *P, uint32_t pt, uint32_t wk, float *x) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) x[k] = k < D ? P[(size_t)pt * D + k] : 0.0f;
+    if (c.jitter[0] != 0.0f || c.jitter[1] != 0.0f || c.jitter[2] != 0.0f) {
+        const uint4 r = philox(c.rng, pt, wk, 0, ROLE_JITTER);
+        x[0] = fmaf(wosm::u01(r.x) - 0.5f, c.jitter[0], x[0]);
+        x[1] = fmaf(wosm::u01(r.y) - 0.5f, c.jitter[1], x[1]);
+        if (D == 3) x[2] = fmaf(wosm::u01(r.z) - 0.5f, c.jitter[2], x[2]);
+    }
+}
+
 // Process the query result at w.p: inside test on the first query, shell
 // test, truncation, then the source term and one step (include/wos.cuh:97-145).
 template <int D>
@@ -277,7 +293,9 @@ __global__ void __launch_bounds__(512) k_walk(SceneView S, WalkCfg c, const floa
                 pt = (uint32_t)(idx / c.nwalks);
                 wk = c.walk_offset + (uint32_t)(idx - (long long)pt * c.nwalks);
             }
-            w.start(P + (size_t)pt * D, D);
+            float x0[3];
+            walk_origin<D>(c, P, pt, wk, x0);
+            w.start(x0, D);
         }
         const Hit hit = warp_queries<D, BVH>(S, active, w.p, w.last, work);
         if (!active) continue;
@@ -344,7 +362,9 @@ __global__ void __launch_bounds__(256) k_walk_plain(SceneView S, WalkCfg c, cons
     const uint32_t pt = (uint32_t)(idx / c.nwalks);
     const uint32_t wk = c.walk_offset + (uint32_t)(idx - (long long)pt * c.nwalks);
     Walker w;
-    w.start(P + (size_t)pt * D, D);
+    float x0[3];
+    walk_origin<D>(c, P, pt, wk, x0);
+    w.start(x0, D);
     Work work{0, 0, 0};
     float v = 0.0f;
     for (;;) {
@@ -723,7 +743,9 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
                 pt = (uint32_t)(idx / c.nwalks);
                 wk = c.walk_offset + (uint32_t)(idx - (long long)pt * c.nwalks);
                 W = (double)__ldg(&dLdu[pt]) / c.nwalks;
-                w.start(P + (size_t)pt * D, D);
+                float x0[3];
+                walk_origin<D>(c, P, pt, wk, x0);
+                w.start(x0, D);
                 phase = PH_PRIMAL;
                 if (W == 0.0) active = false;
                 if (MODE == ADJ_FROM_RECORDS && active) {
@@ -1044,6 +1066,7 @@ WalkCfg make_cfg(const wos_params &p) {
     c.project = p.project_unterminated;
     c.walk_offset = p.walk_offset;
     c.rng = make_rng(p.seed);
+    for (int k = 0; k < 3; ++k) c.jitter[k] = p.jitter[k];
     return c;
 }
 
@@ -1326,7 +1349,9 @@ __global__ void __launch_bounds__(512) k_walk_batch(const SceneView *__restrict_
             const long long local = idx - it.walk_begin;
             pt = (uint32_t)(local / it.nwalks);
             wk = cfgs[item].walk_offset + (uint32_t)(local - (long long)pt * it.nwalks);
-            w.start(it.P + (size_t)pt * D, D);
+            float x0[3];
+            walk_origin<D>(cfgs[item], it.P, pt, wk, x0);
+            w.start(x0, D);
         }
         const Hit hit = warp_queries_batch<D>(views, active, item, w.p, w.last, work);
         if (!active) continue;

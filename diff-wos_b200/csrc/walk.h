@@ -17,6 +17,7 @@ struct WalkCfg {
     uint32_t walk_offset;
     Rng rng;
     int count;  // accumulate LBVH work counters (wos_set_work_counting)
+    float jitter[3];  // start-point jitter extent per axis (0: none)
 };
 
 // Device copy of wos_adjoint_params.

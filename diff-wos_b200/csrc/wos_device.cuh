@@ -125,7 +125,7 @@ __device__ __forceinline__ uint4 philox(Rng key, uint32_t c0, uint32_t c1, uint3
     return make_uint4(c0, c1, c2, c3);
 }
 
-enum { ROLE_PRIMAL = 0, ROLE_ANTI_A = 1, ROLE_ANTI_B = 2, ROLE_EXTRA = 3 };
+enum { ROLE_PRIMAL = 0, ROLE_ANTI_A = 1, ROLE_ANTI_B = 2, ROLE_EXTRA = 3, ROLE_JITTER = 4, ROLE_BOUNDARY = 5 };
 
 // ------------------------------------------------------------------ vectors
 __device__ __forceinline__ float dot2(float ax, float ay, float bx, float by) { return fmaf(ax, bx, ay * by); }

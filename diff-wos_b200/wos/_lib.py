@@ -45,6 +45,7 @@ class WosParams(ctypes.Structure):
         ("use_bvh", ctypes.c_int32),
         ("walk_offset", ctypes.c_uint32),
         ("seed", ctypes.c_uint64),
+        ("jitter", ctypes.c_float * 3),
     ]
 
 

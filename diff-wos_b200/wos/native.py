@@ -56,12 +56,14 @@ class WalkSettings:
     use_bvh: bool = True
     walk_offset: int = 0
     seed: int = 0
+    jitter: tuple = (0.0, 0.0, 0.0)  # start-point jitter extent per axis (pixel sampling)
 
     def c(self) -> WosParams:
+        j = tuple(float(x) for x in self.jitter) + (0.0,) * (3 - len(self.jitter))
         return WosParams(int(self.nwalks), int(self.nsteps), float(self.epsilon), int(self.double_sided),
                          int(self.prevent_fd_artifacts), int(self.use_IS_for_greens), int(self.include_source),
                          int(self.project_unterminated), int(self.use_bvh), int(self.walk_offset) & 0xFFFFFFFF,
-                         int(self.seed) & 0xFFFFFFFFFFFFFFFF)
+                         int(self.seed) & 0xFFFFFFFFFFFFFFFF, (ctypes.c_float * 3)(*j[:3]))
 
 
 @dataclass

@@ -27,6 +27,15 @@ class Detector:
     def size(self):
         return float(np.prod(np.subtract(self.vmax, self.vmin)))
 
+    def pixel(self):
+        """Pixel extent per image axis."""
+        return tuple(float(b - a) / r for a, b, r in zip(self.vmin, self.vmax, self.res))
+
+    def jitter(self):
+        """Start-point jitter of pixel sampling (wos/scene.py:33-39)."""
+        dx, dy = self.pixel()
+        return (dx, dy, 0.0)
+
     def make_points(self) -> torch.Tensor:
         x = torch.linspace(self.vmin[0], self.vmax[0], self.res[0], device="cuda")
         y = torch.linspace(self.vmax[1], self.vmin[1], self.res[1], device="cuda")  # flip y

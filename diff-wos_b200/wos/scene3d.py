@@ -43,6 +43,11 @@ class Detector3DY(Detector):
         y = torch.full((p.shape[0],), float(self.y), device=p.device)
         return torch.stack([p[:, 0], y, p[:, 1]], 1).contiguous()
 
+    def jitter(self):
+        """x and z jitter (wos/scene3d.py:65-71)."""
+        dx, dz = self.pixel()
+        return (dx, 0.0, dz)
+
 
 @dataclass
 class ClosestPointRecord3D:

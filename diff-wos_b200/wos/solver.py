@@ -68,14 +68,15 @@ class Solver:
     include_source = False
     differentiates_source = False
 
-    def walk_settings(self, scene, seed=0, nwalks=None, walk_offset=0) -> WalkSettings:
+    def walk_settings(self, scene, seed=0, nwalks=None, walk_offset=0, jitter=None) -> WalkSettings:
         return WalkSettings(nwalks=int(self.nwalks if nwalks is None else nwalks), nsteps=int(self.nsteps),
                             epsilon=float(self.epsilon), double_sided=bool(self.double_sided),
                             prevent_fd_artifacts=bool(getattr(self, "prevent_fd_artifacts", False)),
                             use_IS_for_greens=bool(getattr(self, "use_IS_for_greens", False)),
                             include_source=bool(self.include_source and scene.source_type != 0),
                             project_unterminated=bool(self.project_unterminated), use_bvh=bool(scene.use_bvh),
-                            walk_offset=int(walk_offset), seed=int(seed))
+                            walk_offset=int(walk_offset), seed=int(seed),
+                            jitter=tuple(jitter) if jitter is not None else (0.0, 0.0, 0.0))
 
     def adjoint_settings(self, scene, want_dV, want_dg, want_dsrc) -> AdjointSettings:
         """Gradients this solver provides as a backward solver: the attached
@@ -85,26 +86,29 @@ class Solver:
                                want_dsrc=bool(want_dsrc and self.differentiates_source))
 
     # ------------------------------------------------------------ primal
-    def solve(self, p, scene, seed=0) -> torch.Tensor:
-        """Per-point means, detached (wos/solver.py:41-44)."""
+    def solve(self, p, scene, seed=0, jitter=None) -> torch.Tensor:
+        """Per-point means, detached (wos/solver.py:41-44).  `jitter`: per-axis
+        extent of a uniform start-point offset per walk (pixel sampling)."""
         P = points(p, scene.dim)
-        return scene._native.solve(P, self.walk_settings(scene, seed)).to(torch.float32)
+        return scene._native.solve(P, self.walk_settings(scene, seed, jitter=jitter)).to(torch.float32)
 
     def solve_stats(self, p, scene, seed=0):
         """(mean, variance of the per-walk values), both float64."""
         P = points(p, scene.dim)
         return scene._native.solve(P, self.walk_settings(scene, seed), want_var=True)
 
-    def walk(self, p, scene, seed=0) -> torch.Tensor:
+    def walk(self, p, scene, seed=0, jitter=None) -> torch.Tensor:
         """Per-point means, attached to the scene's differentiable tensors
         (wos/solver.py:46-65)."""
-        return _attach(self, self, p, scene, seed)
+        return _attach(self, self, p, scene, seed, jitter)
 
     def walk_reduce(self, p, scene, seed=0):
         return self.walk(p, scene, seed)
 
     def walk_detector(self, scene, detector, seed=0):
-        return self.walk(detector.make_points(), scene, seed)
+        """Per-pixel means over nwalks walks, each starting at a uniformly
+        jittered point of its pixel (wos/solver.py:67-84)."""
+        return self.walk(detector.make_points(), scene, seed, jitter=detector.jitter())
 
     def single_walk_preliminary(self, p, scene, sampler):
         """One walk per point; the boundary record (WoS.single_walk in
@@ -149,27 +153,28 @@ class _Job:
     the forward keeps every walk's boundary record and the backward starts
     from it instead of repeating the primal walk (same result)."""
 
-    def __init__(self, fwd, bwd, p, scene, seed, needs=(True, True, True)):
+    def __init__(self, fwd, bwd, p, scene, seed, needs=(True, True, True), jitter=None):
         self.fwd, self.bwd, self.scene, self.seed = fwd, bwd, scene, seed
         self.P = points(p, scene.dim)
         self.records = None
         self.needs = needs
+        self.jitter = jitter
 
     def forward(self):
         if self.fwd is None:
             return torch.zeros(self.P.shape[0], dtype=torch.float32, device=self.P.device)
-        sf = self.fwd.walk_settings(self.scene, self.seed)
-        sb = self.bwd.walk_settings(self.scene, self.seed)
+        sf = self.fwd.walk_settings(self.scene, self.seed, jitter=self.jitter)
+        sb = self.bwd.walk_settings(self.scene, self.seed, jitter=self.jitter)
         if sf == sb:
             a = self.bwd.adjoint_settings(self.scene, *self.needs)
             want_dc = bool(a.want_dsrc and sb.include_source and self.scene.source_type != 0 and self.scene.dim == 2)
             mean, _, rec, dc = self.scene._native.solve_records(self.P, sf, want_dcontrib=want_dc)
             self.records = (rec, dc)
             return mean.to(torch.float32)
-        return self.fwd.solve(self.P, self.scene, self.seed)
+        return self.fwd.solve(self.P, self.scene, self.seed, jitter=self.jitter)
 
     def backward(self, grad, need_V, need_g, need_s):
-        s = self.bwd.walk_settings(self.scene, self.seed)
+        s = self.bwd.walk_settings(self.scene, self.seed, jitter=self.jitter)
         a = self.bwd.adjoint_settings(self.scene, need_V, need_g, need_s)
         if not (a.want_dV or a.want_dg or a.want_dsrc):
             return None, None, None
@@ -203,14 +208,14 @@ class _WalkFunction(torch.autograd.Function):
         return None, dV, dg, ds
 
 
-def _attach(fwd, bwd, p, scene, seed):
+def _attach(fwd, bwd, p, scene, seed, jitter=None):
     tensors = (scene.vertices, scene.values, scene.source_params_tensor())
     if torch.is_grad_enabled() and any(t.requires_grad for t in tensors):
         needs = tuple(bool(t.requires_grad) for t in tensors)
-        return _WalkFunction.apply(_Job(fwd, bwd, p, scene, seed, needs), *tensors)
+        return _WalkFunction.apply(_Job(fwd, bwd, p, scene, seed, needs, jitter), *tensors)
     if fwd is None:
         return torch.zeros(points(p, scene.dim).shape[0], dtype=torch.float32, device=scene.vertices.device)
-    return fwd.solve(p, scene, seed)
+    return fwd.solve(p, scene, seed, jitter=jitter)
 
 
 @dataclass
@@ -220,8 +225,11 @@ class CustomSolver:
     fwd_solver: Solver = None
     bwd_solver: Solver = None
 
-    def walk(self, p, scene, seed=0):
-        return _attach(self.fwd_solver, self.bwd_solver, p, scene, seed)
+    def walk(self, p, scene, seed=0, jitter=None):
+        return _attach(self.fwd_solver, self.bwd_solver, p, scene, seed, jitter)
+
+    def walk_detector(self, scene, detector, seed=0):
+        return self.walk(detector.make_points(), scene, seed, jitter=detector.jitter())
 
     def solve(self, p, scene, seed=0):
         return self.fwd_solver.solve(p, scene, seed)

@@ -43,11 +43,11 @@ class OursCUDA(Solver):
                                want_dV=bool(want_dV), want_dg=bool(want_dg and self.grad_values),
                                want_dsrc=bool(want_dsrc and self.grad_source))
 
-    def walk(self, p, scene, seed=0):
+    def walk(self, p, scene, seed=0, jitter=None):
         """Zero-valued per-point result carrying the gradient."""
-        return _attach(None, self, p, scene, seed)
+        return _attach(None, self, p, scene, seed, jitter)
 
-    def solve(self, p, scene, seed=0):
+    def solve(self, p, scene, seed=0, jitter=None):
         from .fwd import points
         return torch.zeros(points(p, scene.dim).shape[0], dtype=torch.float32, device=scene.vertices.device)
 

@@ -70,7 +70,13 @@ enum {
  *   use_bvh              1: LBVH nearest queries, 0: brute force
  *                        (include/scene.cuh:150-154);
  *   walk_offset          first walk index (the sampler's position);
- *   seed                 64-bit Philox key. */
+ *   seed                 64-bit Philox key;
+ *   jitter               per-axis extent of the start-point jitter: walk w of
+ *                        point i starts at P[i] + (u - 1/2) * jitter with u
+ *                        uniform per axis from the walk's own random numbers
+ *                        (pixel sampling of Solver.walk_detector,
+ *                        wos/solver.py:67-84, wos/scene.py:33-39); zeros
+ *                        start every walk at P[i]. */
 typedef struct wos_params {
     int32_t nwalks;
     int32_t nsteps;
@@ -83,6 +89,7 @@ typedef struct wos_params {
     int32_t use_bvh;
     uint32_t walk_offset;
     uint64_t seed;
+    float jitter[3];
 } wos_params;
 
 /* Settings of the differential estimator (OursCUDA / Ours3D,

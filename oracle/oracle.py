@@ -36,6 +36,7 @@ class Params(ctypes.Structure):
         ("use_bvh", ctypes.c_int32),
         ("walk_offset", ctypes.c_uint32),
         ("seed", ctypes.c_uint64),
+        ("jitter", ctypes.c_float * 3),
     ]
 
 
@@ -54,10 +55,11 @@ class AdjParams(ctypes.Structure):
 
 def make_params(nwalks=1, nsteps=32, epsilon=1e-3, double_sided=False, prevent_fd_artifacts=False,
                 use_IS_for_greens=False, include_source=False, project_unterminated=False, use_bvh=True,
-                walk_offset=0, seed=0) -> Params:
+                walk_offset=0, seed=0, jitter=(0.0, 0.0, 0.0)) -> Params:
+    j = tuple(float(x) for x in jitter) + (0.0,) * (3 - len(jitter))
     return Params(int(nwalks), int(nsteps), float(epsilon), int(double_sided), int(prevent_fd_artifacts),
                   int(use_IS_for_greens), int(include_source), int(project_unterminated), int(use_bvh),
-                  int(walk_offset), int(seed))
+                  int(walk_offset), int(seed), (ctypes.c_float * 3)(*j[:3]))
 
 
 def make_adj(epsilon2=1e-3, clamping=1e-1, control_variates=True, source_in_normal_derivative=False,

@@ -105,6 +105,7 @@ struct Params {
     int32_t use_bvh;
     uint32_t walk_offset;
     uint64_t seed;
+    float jitter[3];
 };
 
 // Must match wos_adjoint_params in include/wos_b200.h.
@@ -119,7 +120,7 @@ struct AdjParams {
     int32_t want_dsrc;
 };
 
-enum { ROLE_PRIMAL = 0, ROLE_ANTI_A = 1, ROLE_ANTI_B = 2, ROLE_EXTRA = 3 };
+enum { ROLE_PRIMAL = 0, ROLE_ANTI_A = 1, ROLE_ANTI_B = 2, ROLE_EXTRA = 3, ROLE_JITTER = 4 };
 
 // ---------------------------------------------------------------- scene
 struct Node {
@@ -742,6 +743,13 @@ static Rec walk(const Scene &S, const float *p0, const Params &prm, float eps, c
     dead.valid = false;
     dead.prim = -1;
     float p[3] = {p0[0], p0[1], D == 3 ? p0[2] : 0.0f};
+    // pixel jitter of the primal walk's start (wos/scene.py:33-39)
+    if (role == ROLE_PRIMAL && (prm.jitter[0] != 0.0f || prm.jitter[1] != 0.0f || prm.jitter[2] != 0.0f)) {
+        const U4 r = rng.draw(pt, wk, 0, ROLE_JITTER);
+        p[0] = fmaf(wosm::u01(r.x) - 0.5f, prm.jitter[0], p[0]);
+        p[1] = fmaf(wosm::u01(r.y) - 0.5f, prm.jitter[1], p[1]);
+        if (D == 3) p[2] = fmaf(wosm::u01(r.z) - 0.5f, prm.jitter[2], p[2]);
+    }
     Hit hit = nearest(S, p, bvh);
     if (steps_out) *steps_out = 0;
     if (!prm.double_sided) {

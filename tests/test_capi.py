@@ -39,7 +39,7 @@ def test_python_binding_covers_header():
 
 def test_struct_layouts():
     from wos import _lib
-    assert ctypes.sizeof(_lib.WosParams) == 48
+    assert ctypes.sizeof(_lib.WosParams) == 64
     assert _lib.WosParams.seed.offset == 40
     assert ctypes.sizeof(_lib.WosAdjointParams) == 32
     assert ctypes.sizeof(_lib.WosLaunchConfig) == 16

@@ -46,7 +46,7 @@ def _settings(**kw):
 def _oparams(oracle, s):
     return oracle.make_params(s.nwalks, s.nsteps, s.epsilon, s.double_sided, s.prevent_fd_artifacts,
                               s.use_IS_for_greens, s.include_source, s.project_unterminated, s.use_bvh,
-                              s.walk_offset, s.seed)
+                              s.walk_offset, s.seed, s.jitter)
 
 
 # ---------------------------------------------------------------- scene build
@@ -124,6 +124,8 @@ WALK_CASES = [
     ("sphere", dict()),
     ("sphere", dict(use_bvh=False, nsteps=8)),
     ("sphere", dict(double_sided=True, nsteps=16)),
+    ("circle", dict(jitter=(0.02, 0.03, 0.0))),
+    ("sphere", dict(jitter=(0.02, 0.0, 0.05))),
 ]
 
 
@@ -243,9 +245,10 @@ def test_device_status_clean(cuda):
 
 
 # ---------------------------------------------------------------- fused path
-@pytest.mark.parametrize("kind,src", [("circle", None), ("star", (2, [0.0, 0.0, 0.0, 0.0, 1.0])),
-                                      ("sphere", None)])
-def test_fused_solve_adjoint_matches_oracle(cuda, oracle, kind, src):
+@pytest.mark.parametrize("kind,src,jitter", [("circle", None, None), ("star", (2, [0.0, 0.0, 0.0, 0.0, 1.0]), None),
+                                             ("sphere", None, None), ("circle", None, (0.05, 0.04, 0.0)),
+                                             ("sphere", None, (0.05, 0.04, 0.0))])
+def test_fused_solve_adjoint_matches_oracle(cuda, oracle, kind, src, jitter):
     from wos.native import AdjointSettings
     if kind == "star":
         V, F, g = star_scene(512)
@@ -254,7 +257,8 @@ def test_fused_solve_adjoint_matches_oracle(cuda, oracle, kind, src):
         V, F, g = {"circle": lambda: circle_scene(256), "sphere": lambda: sphere_scene(2)}[kind]()
         ns, os_ = _scenes(oracle, V, F, g)
     P = _pts2(150, 12, -0.5, 0.5) if V.shape[1] == 2 else _pts3(120, 12, -0.5, 0.5)
-    s = _settings(nwalks=8, nsteps=64, seed=77, include_source=src is not None, use_IS_for_greens=src is not None)
+    s = _settings(nwalks=8, nsteps=64, seed=77, include_source=src is not None, use_IS_for_greens=src is not None,
+                  jitter=jitter or (0.0, 0.0, 0.0))
     a = AdjointSettings(epsilon2=1e-3, clamping=0.1, want_dV=True, want_dg=True, want_dsrc=src is not None)
     out = ns.solve_adjoint(P, s, a, loss_kind=1)
     ov, _, _ = os_.walk_values(P, _oparams(oracle, s))
@@ -317,3 +321,35 @@ def test_autograd_custom_solver_matches_native(cuda, oracle):
     u2 = wos.CustomSolver(fwd, wos.OursCUDA(nwalks=16, nsteps=64, use_IS_for_greens=True)).walk(P, scene, seed=9)
     (u2 * u2).mean().backward()
     assert Vt.grad is not None and gt.grad is None and st.grad is None
+
+
+def test_walk_detector_jittered_pixels(cuda, oracle):
+    """Pixel sampling (wos/solver.py:67-84): each walk starts at a uniformly
+    jittered point of its pixel; the image is the per-pixel mean, and its
+    gradient runs the adjoint from the same jittered starts."""
+    import torch
+    import wos
+    V, F, g = circle_scene(256)
+    Vt = torch.tensor(V, device="cuda", requires_grad=True)
+    scene = wos.Polyline(Vt, F, torch.tensor(g, device="cuda"))
+    det = wos.Detector(vmin=(-0.8, -0.8), vmax=(0.8, 0.8), res=(24, 20))
+    fwd = wos.WoSCUDA(nwalks=8, nsteps=64, epsilon=1e-3)
+    bwd = wos.OursCUDA(nwalks=8, nsteps=64, epsilon=1e-3, epsilon2=1e-3)
+    img = wos.CustomSolver(fwd, bwd).walk_detector(scene, det, seed=3)
+    P = _np(det.make_points())
+    s = fwd.walk_settings(scene, 3, jitter=det.jitter())
+    assert s.jitter == (1.6 / 24, 1.6 / 20, 0.0)
+    os_ = oracle.OracleScene(V, F, g)
+    ov, _, _ = os_.walk_values(P, _oparams(oracle, s))
+    om, _ = oracle.reduce(ov)
+    np.testing.assert_allclose(_np(img), om.astype(np.float32), rtol=1e-6, atol=1e-7)
+    # the jitter changes the walks: unjittered values differ
+    assert not np.array_equal(_np(scene._native.solve(P, fwd.walk_settings(scene, 3))), om)
+    (img * img).sum().backward()
+    dLdu = (2.0 * om).astype(np.float32)
+    a = bwd.adjoint_settings(scene, True, False, False)
+    oa = oracle.make_adj(a.epsilon2, a.clamping, a.control_variates, a.source_in_normal_derivative, a.ball_epsilon,
+                         True, False, False)
+    odV, _, _ = os_.adjoint(P, _oparams(oracle, s), oa, dLdu)
+    np.testing.assert_allclose(_np(Vt.grad), odV, rtol=GRAD_RTOL, atol=GRAD_RTOL * np.abs(odV).max())
+    assert wos.device_status() == 0
