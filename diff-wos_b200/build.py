@@ -23,7 +23,7 @@ BUILD = HERE / "_build"
 LIB = HERE / "lib" / "libwos_b200.so"
 INCLUDE = HERE.parent / "include"
 
-SOURCES = ["scene_build.cu", "walk.cu", "capi.cu", "batch.cu", "noalloc.cu"]
+SOURCES = ["scene_build.cu", "walk.cu", "capi.cu", "batch.cu", "noalloc.cu", "boundary.cu"]
 HEADERS = ["wos_math.h", "wos_device.cuh", "scene_impl.h", "walk.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

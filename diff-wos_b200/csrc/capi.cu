@@ -499,6 +499,110 @@ int wos_solve_adjoint(wos_scene_t scene, const float *P, int n, const wos_params
     return finish_adjoint(S, a, acc, dV, dg, dsrc, st);
 }
 
+size_t wos_solve_tangent_workspace_size(wos_scene_t scene, int n, const wos_params *p, const wos_adjoint_params *a) {
+    if (scene == nullptr || p == nullptr || a == nullptr || n < 0 || p->nwalks < 1) return 0;
+    const SceneImpl &S = scene->impl;
+    const size_t nw = (size_t)n * (size_t)p->nwalks;
+    size_t b = 256;                                                   // queue counter
+    b += align256(sizeof(float) * nw);                                // per-walk values
+    b += align256(wos_walk_record_bytes(S.dim) * nw);                 // per-walk records
+    if (wants_wds(S, *p, *a)) b += align256(sizeof(float) * 5 * nw);  // per-walk source derivatives
+    b += align256(sizeof(float) * nw);                                // per-walk tangents
+    return b;
+}
+
+int wos_solve_tangent(wos_scene_t scene, const float *P, int n, const wos_params *p, const wos_adjoint_params *a,
+                      const float *dV_dir, const float *dg_dir, const float *dsrc_dir, double *mean, double *var,
+                      double *tangent, double *tangent_var, void *workspace, size_t workspace_bytes,
+                      wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (int rc = check_params(p)) return rc;
+    if (int rc = check_adj(a)) return rc;
+    if (n < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "n must be >= 0");
+    if (n == 0) return 0;
+    WOS_CHECK_DEV(P, "P");
+    WOS_CHECK_DEV(mean, "mean");
+    WOS_CHECK_DEV_OPT(var, "var");
+    WOS_CHECK_DEV(tangent, "tangent");
+    WOS_CHECK_DEV_OPT(tangent_var, "tangent_var");
+    WOS_CHECK_DEV_OPT(dV_dir, "dV_dir");
+    WOS_CHECK_DEV_OPT(dg_dir, "dg_dir");
+    WOS_CHECK_DEV_OPT(dsrc_dir, "dsrc_dir");
+    const SceneImpl &S = scene->impl;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t need = wos_solve_tangent_workspace_size(scene, n, p, a);
+    Scratch s;
+    if (int rc = s.init(workspace, workspace_bytes, need, st)) return rc;
+    const size_t nw = (size_t)n * (size_t)p->nwalks;
+    char *b = s.base;
+    unsigned long long *counter = (unsigned long long *)b;
+    b += 256;
+    float *vals = (float *)b;
+    b += align256(sizeof(float) * nw);
+    int *wrec = (int *)b;
+    b += align256(wos_walk_record_bytes(S.dim) * nw);
+    float *wds = nullptr;
+    if (wants_wds(S, *p, *a)) {
+        wds = (float *)b;
+        b += align256(sizeof(float) * 5 * nw);
+    }
+    float *tan = (float *)b;
+    cudaError_t e = cudaMemsetAsync(tan, 0, sizeof(float) * nw, st);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(tangents)");
+    WalkOut o{vals, nullptr, wrec, wds, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    if (int rc = launch_walk(S, P, (long long)nw, *p, false, o, counter, st)) return rc;
+    if (int rc = launch_reduce(vals, n, p->nwalks, mean, var, st)) return rc;
+    AdjOut ao{};
+    ao.wrec = wrec;
+    ao.wds = wds;
+    ao.tV = dV_dir;
+    ao.tg = dg_dir;
+    ao.ts = dsrc_dir;
+    ao.tan = tan;
+    if (int rc = launch_adjoint(S, P, (long long)nw, *p, make_adj(*a), nullptr, ADJ_TANGENT, ao, counter, st))
+        return rc;
+    return launch_reduce(tan, n, p->nwalks, tangent, tangent_var, st);
+}
+
+int wos_boundary_term(wos_scene_t scene, const wos_detector *det, int nwalks, uint64_t seed, const float *dV_dir,
+                      double *image_tangent, const float *dLdI, float *dV, wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (det == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "detector is NULL");
+    if (nwalks < 1) return fail(WOS_ERR_INVALID_ARGUMENT, "nwalks must be >= 1");
+    const SceneImpl &S = scene->impl;
+    if (det->res[0] < 1 || det->res[1] < 1) return fail(WOS_ERR_INVALID_ARGUMENT, "detector res must be >= 1");
+    if (!(det->vmax[0] > det->vmin[0]) || !(det->vmax[1] > det->vmin[1]))
+        return fail(WOS_ERR_INVALID_ARGUMENT, "detector vmax must exceed vmin");
+    if (det->axis_u < 0 || det->axis_u >= S.dim || det->axis_v < 0 || det->axis_v >= S.dim ||
+        det->slab_axis < -1 || det->slab_axis >= S.dim)
+        return fail(WOS_ERR_INVALID_ARGUMENT, "detector axes out of range for the scene's dimension");
+    if (!(det->size > 0.0f)) return fail(WOS_ERR_INVALID_ARGUMENT, "detector size must be > 0");
+    if ((dV_dir == nullptr) != (image_tangent == nullptr))
+        return fail(WOS_ERR_INVALID_ARGUMENT, "dV_dir and image_tangent go together");
+    if ((dLdI == nullptr) != (dV == nullptr)) return fail(WOS_ERR_INVALID_ARGUMENT, "dLdI and dV go together");
+    WOS_CHECK_DEV_OPT(dV_dir, "dV_dir");
+    WOS_CHECK_DEV_OPT(image_tangent, "image_tangent");
+    WOS_CHECK_DEV_OPT(dLdI, "dLdI");
+    WOS_CHECK_DEV_OPT(dV, "dV");
+    if (dV_dir == nullptr && dLdI == nullptr) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    double *acc = nullptr;
+    const long long nvd = (long long)S.nV * S.dim;
+    if (dV != nullptr) {
+        cudaError_t e = cudaMallocAsync((void **)&acc, sizeof(double) * (size_t)std::max<long long>(nvd, 1), st);
+        if (e != cudaSuccess) return fail_cuda(e, "cudaMallocAsync(boundary accumulators)");
+        e = cudaMemsetAsync(acc, 0, sizeof(double) * (size_t)nvd, st);
+        if (e != cudaSuccess) {
+            cudaFreeAsync(acc, st);
+            return fail_cuda(e, "cudaMemsetAsync(boundary accumulators)");
+        }
+    }
+    int rc = launch_boundary(S, *det, nwalks, seed, dV_dir, image_tangent, dLdI, acc, st);
+    if (rc == 0 && acc != nullptr) rc = launch_add_f64(acc, dV, nvd, st);
+    if (acc != nullptr) cudaFreeAsync(acc, st);
+    return rc;
+}
+
 int wos_solve_records(wos_scene_t scene, const float *P, int n, const wos_params *p, double *mean, double *var,
                       void *records, float *dcontrib, void *workspace, size_t workspace_bytes, wos_stream_t stream) {
     if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");

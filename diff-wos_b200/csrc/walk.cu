@@ -664,6 +664,7 @@ struct AdjSlot {
     float ba, bb;  // bisection bracket
     int bk;
     int bwarm;     // primitive that blocked the last rejected radius, or -1
+    float tacc;    // tangent mode: the sample's directional derivative so far
     double acc[5];  // source-parameter gradient accumulators
 };
 constexpr int ADJ_THREAD_WORDS = (int)((sizeof(AdjSlot) + 7) / 8);
@@ -700,6 +701,9 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
     int &bwarm = slot.bwarm;
     const bool src2 = D == 2 && S.src_type != 0;
     constexpr bool ND_ONLY = MODE == ADJ_ND_ONLY;
+    constexpr bool TAN = MODE == ADJ_TANGENT;
+    constexpr bool FROM_REC = MODE == ADJ_FROM_RECORDS || TAN;
+    float &tacc = slot.tacc;
     const bool want_src = !ND_ONLY && a.want_dsrc && c.include_source && src2;
     const bool with_src = a.source_in_nd && src2;
     Queue q{0, 0, false};
@@ -742,13 +746,14 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
             } else {
                 pt = (uint32_t)(idx / c.nwalks);
                 wk = c.walk_offset + (uint32_t)(idx - (long long)pt * c.nwalks);
-                W = (double)__ldg(&dLdu[pt]) / c.nwalks;
+                W = TAN ? 1.0 : (double)__ldg(&dLdu[pt]) / c.nwalks;
                 float x0[3];
                 walk_origin<D>(c, P, pt, wk, x0);
                 w.start(x0, D);
                 phase = PH_PRIMAL;
+                tacc = 0.0f;
                 if (W == 0.0) active = false;
-                if (MODE == ADJ_FROM_RECORDS && active) {
+                if (FROM_REC && active) {
                     // the primal walk ran in the forward pass: start from its record
                     int code;
                     if (D == 2) {
@@ -770,16 +775,29 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
                         int vid[3];
                         float wts[3];
                         st.uref = dirichlet<D>(S, rprim, rt0, rt1, vid, wts);
-                        if (a.want_dg) {
+                        if (TAN) {
+                            if (a.want_dg && out.tg != nullptr) {
 #pragma unroll
-                            for (int s2 = 0; s2 < D; ++s2) atomicAdd(&out.dg[vid[s2]], W * (double)wts[s2]);
-                        }
-                        if (want_src) {
+                                for (int s2 = 0; s2 < D; ++s2) tacc = fmaf(wts[s2], __ldg(&out.tg[vid[s2]]), tacc);
+                            }
+                            if (want_src && out.ts != nullptr) {
 #pragma unroll
-                            for (int k = 0; k < 5; ++k)
-                                acc_src[k] += W * (double)__ldg(&out.wds[(size_t)idx * 5 + k]);
+                                for (int k = 0; k < 5; ++k)
+                                    tacc = fmaf(__ldg(&out.wds[(size_t)idx * 5 + k]), __ldg(&out.ts[k]), tacc);
+                            }
+                        } else {
+                            if (a.want_dg) {
+#pragma unroll
+                                for (int s2 = 0; s2 < D; ++s2) atomicAdd(&out.dg[vid[s2]], W * (double)wts[s2]);
+                            }
+                            if (want_src) {
+#pragma unroll
+                                for (int k = 0; k < 5; ++k)
+                                    acc_src[k] += W * (double)__ldg(&out.wds[(size_t)idx * 5 + k]);
+                            }
                         }
-                        if (!a.want_dV) {
+                        if (!a.want_dV || (TAN && out.tV == nullptr)) {
+                            if (TAN) out.tan[idx] = tacc;
                             active = false;
                         } else {
 #pragma unroll
@@ -944,18 +962,28 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
                 int vid[3];
                 float wts[3];
                 dirichlet<D>(S, rprim, rt0, rt1, vid, wts);
+                if (TAN) {
+                    // d(sample) = -(grad_n + grad_t) . dx, dx = sum_s wts_s dV[vid_s]
 #pragma unroll
-                for (int s = 0; s < D; ++s)
+                    for (int s = 0; s < D; ++s)
 #pragma unroll
-                    for (int k = 0; k < D; ++k)
-                        atomicAdd(&out.dV[(size_t)vid[s] * D + k], W * (double)(-(wts[s] * (gn[k] + gt[k]))));
+                        for (int k = 0; k < D; ++k)
+                            tacc = fmaf(-(wts[s] * (gn[k] + gt[k])), __ldg(&out.tV[(size_t)vid[s] * D + k]), tacc);
+                    out.tan[idx] = tacc;
+                } else {
+#pragma unroll
+                    for (int s = 0; s < D; ++s)
+#pragma unroll
+                        for (int k = 0; k < D; ++k)
+                            atomicAdd(&out.dV[(size_t)vid[s] * D + k], W * (double)(-(wts[s] * (gn[k] + gt[k]))));
+                }
             }
             active = false;
             phase = PH_IDLE;
         }
     }
     if (c.count) flush_work<BVH>(work);
-    if (want_src) {
+    if (want_src && !TAN) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
             double v = acc_src[k];
@@ -1238,11 +1266,13 @@ int launch_adjoint(const SceneImpl &S, const float *P, long long total, const wo
     if (total == 0) return 0;
     const bool bvh = p.use_bvh != 0;
 #define WOS_ADJ(D_, B_)                                                                                       \
-    return mode == ADJ_ND_ONLY                                                                                \
-               ? launch_adjoint_t<D_, B_, ADJ_ND_ONLY>(S, P, total, p, a, dLdu, out, counter, st)            \
-               : (mode == ADJ_FROM_RECORDS                                                                    \
-                      ? launch_adjoint_t<D_, B_, ADJ_FROM_RECORDS>(S, P, total, p, a, dLdu, out, counter, st) \
-                      : launch_adjoint_t<D_, B_, ADJ_RECOMPUTE>(S, P, total, p, a, dLdu, out, counter, st))
+    switch (mode) {                                                                                           \
+        case ADJ_ND_ONLY: return launch_adjoint_t<D_, B_, ADJ_ND_ONLY>(S, P, total, p, a, dLdu, out, counter, st); \
+        case ADJ_FROM_RECORDS:                                                                                \
+            return launch_adjoint_t<D_, B_, ADJ_FROM_RECORDS>(S, P, total, p, a, dLdu, out, counter, st);     \
+        case ADJ_TANGENT: return launch_adjoint_t<D_, B_, ADJ_TANGENT>(S, P, total, p, a, dLdu, out, counter, st); \
+        default: return launch_adjoint_t<D_, B_, ADJ_RECOMPUTE>(S, P, total, p, a, dLdu, out, counter, st);  \
+    }
     if (S.dim == 2) {
         if (bvh) WOS_ADJ(2, true);
         WOS_ADJ(2, false);

@@ -55,9 +55,16 @@ struct AdjOut {
     // records mode: per-walk WalkRec and source derivatives from the forward pass
     const int *wrec;
     const float *wds;
+    // tangent mode: directions of vertices (nV x dim), values (nV) and source
+    // parameters (5), each may be null; per-walk directional derivative out
+    const float *tV, *tg, *ts;
+    float *tan;
 };
 
-enum AdjMode { ADJ_RECOMPUTE = 0, ADJ_ND_ONLY = 1, ADJ_FROM_RECORDS = 2 };
+// ADJ_TANGENT: forward mode from records -- each walk's derivative along a
+// direction of (vertices, values, source parameters) instead of the scatter
+// of dL/du into their gradients.
+enum AdjMode { ADJ_RECOMPUTE = 0, ADJ_ND_ONLY = 1, ADJ_FROM_RECORDS = 2, ADJ_TANGENT = 3 };
 
 // One (scene, query set) item of a batched launch, in device memory.
 struct BatchItemDev {
@@ -108,5 +115,10 @@ int launch_adjoint(const SceneImpl &S, const float *P, long long total, const wo
 int launch_loss(const double *mean, int n, int kind, const float *target_or_dLdu, float *dLdu, double *loss,
                 cudaStream_t st);
 int launch_add_f64(const double *src, float *dst, long long n, cudaStream_t st);
+// Image-space boundary term (boundary.cu): forward mode into img_tan
+// (npixels doubles, added) for vertex motion tV, and / or reverse mode into
+// dV_acc (nV x dim doubles, added) for pixel weights dLdI.
+int launch_boundary(const SceneImpl &S, const wos_detector &d, int nwalks, uint64_t seed, const float *tV,
+                    double *img_tan, const float *dLdI, double *dV_acc, cudaStream_t st);
 
 }  // namespace wosd

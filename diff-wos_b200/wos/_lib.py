@@ -85,6 +85,20 @@ class WosLaunchConfig(ctypes.Structure):
     ]
 
 
+class WosDetector(ctypes.Structure):
+    _fields_ = [
+        ("vmin", ctypes.c_float * 2),
+        ("vmax", ctypes.c_float * 2),
+        ("res", ctypes.c_int32 * 2),
+        ("axis_u", ctypes.c_int32),
+        ("axis_v", ctypes.c_int32),
+        ("slab_axis", ctypes.c_int32),
+        ("slab_center", ctypes.c_float),
+        ("slab_half_width", ctypes.c_float),
+        ("size", ctypes.c_float),
+    ]
+
+
 class WosBatchItem(ctypes.Structure):
     _fields_ = [
         ("scene", ctypes.c_void_p),
@@ -137,6 +151,13 @@ SIGNATURES = {
          _P],
     ),
     "wos_solve_adjoint_workspace_size": (_S, [_P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams)]),
+    "wos_boundary_term": (_I, [_P, ctypes.POINTER(WosDetector), _I, ctypes.c_uint64, _P, _P, _P, _P, _P]),
+    "wos_solve_tangent_workspace_size": (_S, [_P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams)]),
+    "wos_solve_tangent": (
+        _I,
+        [_P, _P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams), _P, _P, _P, _P, _P, _P, _P, _P, _S,
+         _P],
+    ),
     "wos_solve_adjoint": (
         _I,
         [_P, _P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams), _I, _P, _P, _P, _P, _P, _P, _P,

@@ -287,6 +287,55 @@ class NativeScene:
                  workspace.data_ptr(), need, stream())
         return dict(mean=mean, var=var, loss=loss, dV=dV, dg=dg, dsrc=ds)
 
+    def solve_tangent(self, P, s: WalkSettings, a: AdjointSettings, dV=None, dg=None, dsrc=None, want_var=False,
+                      workspace: torch.Tensor | None = None):
+        """Fused forward solve + forward-mode derivative of the per-point means
+        along the direction (dV: nV x dim, dg: nV, dsrc: 5; None = still)."""
+        P = as_cuda(P, torch.float32, self.dim)
+        n = int(P.shape[0])
+        d = self.device
+        mean = torch.empty(n, dtype=torch.float64, device=d)
+        tan = torch.empty(n, dtype=torch.float64, device=d)
+        var = torch.empty(n, dtype=torch.float64, device=d) if want_var else None
+        tvar = torch.empty(n, dtype=torch.float64, device=d) if want_var else None
+        tV = as_cuda(dV, torch.float32, self.dim) if dV is not None else None
+        if tV is not None and tV.shape[0] != self.nV:
+            raise ValueError("dV must be nV x dim")
+        tg = as_cuda(dg, torch.float32).reshape(-1) if dg is not None else None
+        if tg is not None and tg.numel() != self.nV:
+            raise ValueError("dg must have one entry per vertex")
+        ts = as_cuda(dsrc, torch.float32).reshape(-1) if dsrc is not None else None
+        if ts is not None and ts.numel() != 5:
+            raise ValueError("dsrc must have 5 entries")
+        if n:
+            c, ca = s.c(), a.c()
+            need = _lib.lib().wos_solve_tangent_workspace_size(self.h, n, ctypes.byref(c), ctypes.byref(ca))
+            if workspace is None or workspace.numel() < need:
+                workspace = torch.empty(need, dtype=torch.uint8, device=d)
+            call("wos_solve_tangent", self.h, P.data_ptr(), n, ctypes.byref(c), ctypes.byref(ca), _ptr(tV), _ptr(tg),
+                 _ptr(ts), mean.data_ptr(), _ptr(var), tan.data_ptr(), _ptr(tvar), workspace.data_ptr(), need,
+                 stream())
+        return dict(mean=mean, var=var, tangent=tan, tangent_var=tvar)
+
+    def boundary_term(self, det, nwalks: int, seed: int = 0, dV_dir=None, dLdI=None):
+        """Image-space boundary term (wos_boundary_term): the derivative image
+        for vertex motion dV_dir (forward mode) and / or the vertex gradient
+        of pixel weights dLdI (reverse mode).  `det` is a WosDetector.
+        Returns (image_tangent or None, dV or None)."""
+        npix = int(det.res[0]) * int(det.res[1])
+        d = self.device
+        tV = as_cuda(dV_dir, torch.float32, self.dim) if dV_dir is not None else None
+        if tV is not None and tV.shape[0] != self.nV:
+            raise ValueError("dV_dir must be nV x dim")
+        w = as_cuda(dLdI, torch.float32).reshape(-1) if dLdI is not None else None
+        if w is not None and w.numel() != npix:
+            raise ValueError("dLdI must have one entry per pixel")
+        img = torch.zeros(npix, dtype=torch.float64, device=d) if tV is not None else None
+        dV = torch.zeros((self.nV, self.dim), dtype=torch.float32, device=d) if w is not None else None
+        call("wos_boundary_term", self.h, ctypes.byref(det), int(nwalks), int(seed) & 0xFFFFFFFFFFFFFFFF, _ptr(tV),
+             _ptr(img), _ptr(w), _ptr(dV), stream())
+        return img, dV
+
     def normal_derivative(self, rec, s: WalkSettings, a: AdjointSettings) -> torch.Tensor:
         valid = as_cuda(rec["valid"], torch.uint8).reshape(-1)
         n = int(valid.numel())

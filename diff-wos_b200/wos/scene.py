@@ -8,6 +8,8 @@ solvers differentiate through them (values, source_params, vertices).
 """
 from __future__ import annotations
 
+import ctypes
+
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -35,6 +37,12 @@ class Detector:
         """Start-point jitter of pixel sampling (wos/scene.py:33-39)."""
         dx, dy = self.pixel()
         return (dx, dy, 0.0)
+
+    def c(self):
+        """The detector for the C ABI (wos_detector)."""
+        from ._lib import WosDetector
+        return WosDetector((ctypes.c_float * 2)(*self.vmin), (ctypes.c_float * 2)(*self.vmax),
+                           (ctypes.c_int32 * 2)(*self.res), 0, 1, -1, 0.0, 0.0, float(self.size()))
 
     def make_points(self) -> torch.Tensor:
         x = torch.linspace(self.vmin[0], self.vmax[0], self.res[0], device="cuda")

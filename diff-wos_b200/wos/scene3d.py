@@ -28,6 +28,12 @@ class Detector3D(Detector):
         z = torch.full((p.shape[0], 1), float(self.z), device=p.device)
         return torch.cat([p, z], 1).contiguous()
 
+    def c(self):
+        """Slab |z - self.z| < l_z / 2 (wos/scene3d.py:35-41)."""
+        d = super().c()
+        d.slab_axis, d.slab_center, d.slab_half_width = 2, float(self.z), float(self.l_z) / 2
+        return d
+
 
 @dataclass
 class Detector3DY(Detector):
@@ -47,6 +53,17 @@ class Detector3DY(Detector):
         """x and z jitter (wos/scene3d.py:65-71)."""
         dx, dz = self.pixel()
         return (dx, 0.0, dz)
+
+    def size(self):
+        """Slab volume (image area x l_y)."""
+        return float(np.prod(np.subtract(self.vmax, self.vmin))) * self.l_y
+
+    def c(self):
+        """Image axes x, z; slab |y - self.y| < l_y / 2 (wos/scene3d.py:73-81)."""
+        d = super().c()
+        d.axis_u, d.axis_v = 0, 2
+        d.slab_axis, d.slab_center, d.slab_half_width = 1, float(self.y), float(self.l_y) / 2
+        return d
 
 
 @dataclass

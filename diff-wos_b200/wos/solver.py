@@ -173,6 +173,18 @@ class _Job:
             return mean.to(torch.float32)
         return self.fwd.solve(self.P, self.scene, self.seed, jitter=self.jitter)
 
+    def tangent(self, dV, dg, ds):
+        """Forward mode: derivative of the per-point means along (dV, dg, ds)
+        (any may be None), from the backward solver's estimator with the same
+        seed (wos_solve_tangent)."""
+        s = self.bwd.walk_settings(self.scene, self.seed, jitter=self.jitter)
+        a = self.bwd.adjoint_settings(self.scene, dV is not None, dg is not None, ds is not None)
+        if not (a.want_dV or a.want_dg or a.want_dsrc):
+            return torch.zeros(self.P.shape[0], dtype=torch.float32, device=self.P.device)
+        out = self.scene._native.solve_tangent(self.P, s, a, dV=dV if a.want_dV else None,
+                                               dg=dg if a.want_dg else None, dsrc=ds if a.want_dsrc else None)
+        return out["tangent"].to(torch.float32)
+
     def backward(self, grad, need_V, need_g, need_s):
         s = self.bwd.walk_settings(self.scene, self.seed, jitter=self.jitter)
         a = self.bwd.adjoint_settings(self.scene, need_V, need_g, need_s)
@@ -207,11 +219,20 @@ class _WalkFunction(torch.autograd.Function):
         ds = ds.reshape(ctx.shapes[2]) if (ns and ds is not None) else None
         return None, dV, dg, ds
 
+    @staticmethod
+    def jvp(ctx, _job, dV, dg, ds):
+        return ctx.job.tangent(dV, dg, ds)
+
+
+def has_tangent(t) -> bool:
+    """True for a forward-mode dual tensor (torch.autograd.forward_ad)."""
+    return isinstance(t, torch.Tensor) and torch.autograd.forward_ad.unpack_dual(t).tangent is not None
+
 
 def _attach(fwd, bwd, p, scene, seed, jitter=None):
     tensors = (scene.vertices, scene.values, scene.source_params_tensor())
-    if torch.is_grad_enabled() and any(t.requires_grad for t in tensors):
-        needs = tuple(bool(t.requires_grad) for t in tensors)
+    if any(has_tangent(t) for t in tensors) or (torch.is_grad_enabled() and any(t.requires_grad for t in tensors)):
+        needs = tuple(bool(t.requires_grad) or has_tangent(t) for t in tensors)
         return _WalkFunction.apply(_Job(fwd, bwd, p, scene, seed, needs, jitter), *tensors)
     if fwd is None:
         return torch.zeros(points(p, scene.dim).shape[0], dtype=torch.float32, device=scene.vertices.device)

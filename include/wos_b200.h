@@ -269,6 +269,59 @@ WOS_API int wos_solve_adjoint(wos_scene_t scene, const float *P, int n, const wo
                               double *var, double *loss, float *dV, float *dg, float *dsrc, void *workspace,
                               size_t workspace_bytes, wos_stream_t stream);
 
+/* Workspace of wos_solve_tangent. */
+WOS_API size_t wos_solve_tangent_workspace_size(wos_scene_t scene, int n, const wos_params *p,
+                                                const wos_adjoint_params *a);
+
+/* Fused forward solve + forward-mode derivative of the per-point means along
+ * a direction of the scene: dV_dir (nV x dim), dg_dir (nV) and dsrc_dir (5),
+ * each may be NULL (no motion of that input; also skipped unless the
+ * matching want_* flag of `a` is set).  tangent[i] (and tangent_var[i], may
+ * be NULL) receive the mean (and sample variance) over point i's walks of
+ * each walk's directional derivative: the boundary-shape term
+ * -(grad_n u + grad_t g) . dx with dx the motion of the walk's boundary point,
+ * plus the Dirichlet gather and the source term.  This is what the
+ * reference's forward-mode renderings compute (dr.forward_to on a scene
+ * parameter, diff_solve/runner.py:75-109); the estimator is the same as
+ * wos_solve_adjoint's, so tangent summed against weights equals the adjoint
+ * of that weighting dotted with the direction. */
+WOS_API int wos_solve_tangent(wos_scene_t scene, const float *P, int n, const wos_params *p,
+                              const wos_adjoint_params *a, const float *dV_dir, const float *dg_dir,
+                              const float *dsrc_dir, double *mean, double *var, double *tangent, double *tangent_var,
+                              void *workspace, size_t workspace_bytes, wos_stream_t stream);
+
+/* A detector: res[0] x res[1] pixels over [vmin, vmax] in scene axes
+ * (axis_u, axis_v); in 3D a slab |x[slab_axis] - slab_center| <
+ * slab_half_width (slab_axis -1 in 2D); size = its area (2D) or slab volume
+ * (3D) (Detector / Detector3D / Detector3DY, wos/scene.py:9-42,
+ * wos/scene3d.py:9-85).  Pixel of a point: u = (x[axis_u] - vmin[0]) /
+ * (vmax[0] - vmin[0]) * res[0] + 0.5 truncated, likewise v, index
+ * u + (res[1] - v) * res[0] (the reference's Detector.index); points whose
+ * index falls outside the image are dropped. */
+typedef struct wos_detector {
+    float vmin[2];
+    float vmax[2];
+    int32_t res[2];
+    int32_t axis_u, axis_v;
+    int32_t slab_axis;
+    float slab_center, slab_half_width;
+    float size;
+} wos_detector;
+
+/* Image-space boundary term of the shape derivative (WoSBoundary,
+ * wos/wos_boundary.py:11-31): res[0] * res[1] * nwalks boundary points drawn
+ * uniformly by length (2D) or area (3D) with Philox(seed); each contributes
+ * -g(x) (n . dx) / pdf / (size * nwalks) to its pixel, n the primitive's
+ * normal (-ab.y, ab.x)/|ab| in 2D and -(ab x ac)/|ab x ac| in 3D, dx the
+ * motion of the sampled point.  Forward mode: dV_dir (nV x dim) and
+ * image_tangent (npixels doubles, added to).  Reverse mode: dLdI (npixels)
+ * and dV (nV x dim floats, added to).  Either pair may be NULL.  The 3D pdf
+ * is 1 / (total area); the reference divides the triangle pmf by |ab x ac|,
+ * twice the area, which doubles its 3D term. */
+WOS_API int wos_boundary_term(wos_scene_t scene, const wos_detector *det, int nwalks, uint64_t seed,
+                              const float *dV_dir, double *image_tangent, const float *dLdI, float *dV,
+                              wos_stream_t stream);
+
 /* ---------------------------------------------------------------- batched */
 
 /* One (scene, query set) of a batch.  P (n x dim) and target_or_dLdu stay at
