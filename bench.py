@@ -413,7 +413,7 @@ def c3_main(args):
     dev = torch.device("cuda", local)
     V, F = shapes.displaced_icosphere(6, 0.15, seed=0)
     scene = NativeScene(V, F, shapes.harmonic_c3(V).astype(np.float32))
-    npts, nw = args.points, args.walks if args.walks != NWALKS else 128
+    npts, nw = args.points, args.walks if args.walks is not None else 128
     cand = shapes.sample_interior_3d(int(npts * 1.1) + 1024, shapes.displaced_radius_fn(0.15, 0), seed=1,
                                      margin=0.005)
     ins = scene.closest(cand, True, want=("inside",))["inside"].cpu().numpy().astype(bool)
@@ -572,7 +572,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ref-step-s", type=float, default=6.0)
     ap.add_argument("--grid", type=int, default=GRID, help="query grid (smaller only for profiling captures)")
-    ap.add_argument("--walks", type=int, default=NWALKS, help="walks per point (smaller only for profiling)")
+    ap.add_argument("--walks", type=int, default=None,
+                    help="walks per point (c2: 256, c3: 128; smaller only for profiling)")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "batched"],
                     help="c2: the 2D differentiable solve (default); c3: the 3D forward + adjoint solve; "
                          "c4: the 2D inverse problem; batched: many scenes in one launch")
@@ -580,7 +581,7 @@ def main():
     ap.add_argument("--points", type=int, default=1_000_000, help="query points of the c3 workload")
     ap.add_argument("--scale", type=float, default=0.1, help="query-count scale of the batched workload")
     args = ap.parse_args()
-    set_size(args.grid, args.walks)
+    set_size(args.grid, args.walks if args.walks is not None else NWALKS)
     if args.workload == "batched" and args.impl == "ours":
         return batched_main(args)
     if args.workload == "c3" and args.impl == "ours":
