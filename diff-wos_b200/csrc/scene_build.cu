@@ -155,10 +155,50 @@ __device__ __forceinline__ uint32_t spread3(uint32_t x) {
     return x;
 }
 
-// Primitive precomputation, primitive boxes and Morton keys.
+// Hilbert index of a 3D cell (10 bits per axis), by Skilling's transpose
+// method ("Programming the Hilbert curve", AIP Conf. Proc. 707, 2004): undo
+// the excess work of the axes, Gray-encode, then interleave the transposed
+// bits, axis 0 most significant.  Consecutive indices are face-adjacent
+// cells, so runs of primitives sorted by it are more compact than Morton
+// runs, whose curve jumps between octants.
+__device__ __forceinline__ uint32_t hilbert3(uint32_t x0, uint32_t x1, uint32_t x2) {
+    uint32_t X[3] = {x0, x1, x2};
+    const uint32_t M = 1u << 9;
+    for (uint32_t Q = M; Q > 1; Q >>= 1) {
+        const uint32_t P = Q - 1;
+        for (int i = 0; i < 3; ++i) {
+            if (X[i] & Q) {
+                X[0] ^= P;
+            } else {
+                const uint32_t t = (X[0] ^ X[i]) & P;
+                X[0] ^= t;
+                X[i] ^= t;
+            }
+        }
+    }
+    X[1] ^= X[0];
+    X[2] ^= X[1];
+    uint32_t t = 0;
+    for (uint32_t Q = M; Q > 1; Q >>= 1)
+        if (X[2] & Q) t ^= Q - 1;
+    for (int i = 0; i < 3; ++i) X[i] ^= t;
+    return (spread3(X[0]) << 2) | (spread3(X[1]) << 1) | spread3(X[2]);
+}
+
+// Number of segments f whose end vertex starts segment f + 1 (cyclically).
+__global__ void k_chain_count(const int *F, int nF, int *count) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    const int next = f + 1 < nF ? f + 1 : 0;
+    if (F[2 * f + 1] == F[2 * next]) atomicAdd(count, 1);
+}
+
+// Primitive precomputation, primitive boxes and sort keys: Morton (order 0),
+// the input index (order 1) or Hilbert (order 2) of the box centre.
 template <int D>
 __global__ void k_prims(const float *V, const int *F, int nF, float lo0, float lo1, float lo2, float hi0, float hi1,
-                        float hi2, float4 *seg, float *seginv, float4 *tri, float *pbox, unsigned long long *keys) {
+                        float hi2, float4 *seg, float *seginv, float4 *tri, float *pbox, unsigned long long *keys,
+                        int order) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= nF) return;
     const float slo[3] = {lo0, lo1, lo2}, shi[3] = {hi0, hi1, hi2};
@@ -205,8 +245,14 @@ __global__ void k_prims(const float *V, const int *F, int nF, float lo0, float l
         const float u = ext > 0.0f ? (c - slo[k]) / ext : 0.0f;
         q[k] = (uint32_t)fminf(fmaxf(u * scale, 0.0f), scale - 1.0f);
     }
-    const uint32_t m = D == 2 ? (spread2(q[0]) | (spread2(q[1]) << 1))
-                              : (spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2));
+    uint32_t m;
+    if (order == 1)
+        m = (uint32_t)f;
+    else if (D == 3 && order == 2)
+        m = hilbert3(q[0], q[1], q[2]);
+    else
+        m = D == 2 ? (spread2(q[0]) | (spread2(q[1]) << 1))
+                   : (spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2));
     keys[f] = ((unsigned long long)m << 32) | (unsigned)f;
 }
 
@@ -604,14 +650,33 @@ static int build_geometry(SceneImpl &S, cudaStream_t st) {
         cudaFreeAsync(end, st);
     }
 
-    // ---- primitives + Morton keys
+    // ---- primitive order: a polyline whose segments follow each other keeps
+    // its input order (its leaves are then arcs of the curve, the most
+    // compact runs); other polylines sort by Morton code, meshes by Hilbert
+    // index.  Decided once: moving vertices keeps the order.
+    if (S.prim_order < 0) {
+        S.prim_order = D == 3 ? 2 : 0;
+        if (D == 2 && nF >= 2) {
+            int *cnt = nullptr;
+            WOS_TRY(dalloc(&cnt, 1, st));
+            WOS_TRY(cudaMemsetAsync(cnt, 0, sizeof(int), st));
+            k_chain_count<<<nblk(nF, TB), TB, 0, st>>>(S.F, nF, cnt);
+            int cnt_h = 0;
+            WOS_TRY(cudaMemcpyAsync(&cnt_h, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+            WOS_TRY(cudaStreamSynchronize(st));
+            cudaFreeAsync(cnt, st);
+            if (cnt_h >= nF - nF / 10) S.prim_order = 1;
+        }
+    }
+
+    // ---- primitives + sort keys
     float *pbox = nullptr;
     unsigned long long *mkeys = nullptr, *skeys = nullptr;
     WOS_TRY(dalloc(&pbox, (size_t)nF * 2 * D, st));
     WOS_TRY(dalloc(&mkeys, nF, st));
     WOS_TRY(dalloc(&skeys, nF, st));
     k_prims<D><<<nblk(nF, TB), TB, 0, st>>>(S.V, S.F, nF, S.lo[0], S.lo[1], S.lo[2], S.hi[0], S.hi[1], S.hi[2], S.seg,
-                                           S.seginv, S.tri, pbox, mkeys);
+                                           S.seginv, S.tri, pbox, mkeys, S.prim_order);
     {
         size_t tmp_bytes = 0;
         cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, mkeys, skeys, nF, 0, 64, st);

@@ -33,6 +33,10 @@ struct SceneImpl {
     float4 *tri = nullptr;
     int nNodes = 0;
     int depth = 0;
+    // Primitive order of the trees (decided at the first build, kept when
+    // vertices move): 0 Morton, 1 input order (a polyline whose segments
+    // follow each other), 2 Hilbert.
+    int prim_order = -1;
     float4 *node = nullptr;
     float4 *lseg = nullptr;
     float *lseginv = nullptr;
