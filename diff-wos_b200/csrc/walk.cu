@@ -532,41 +532,47 @@ __device__ __forceinline__ float eval_P(const float *c, const float *y, const fl
 }
 
 // State of one normal-derivative sample on the inscribed ball of radius R
-// centred at c (wos/wos.py:196-232, wos/wos3d.py:254-286).
+// centred at c = p + rn R (wos/wos.py:196-232, wos/wos3d.py:254-286).  The
+// outward normal n = -rn, the centre and the second tangent are recomputed
+// where needed (the same float operations as storing them), which keeps the
+// per-thread state small.
 struct NdState {
-    float n[3];    // outward normal (-record normal)
     float p[3];    // boundary point
-    float c[3];    // ball centre
+    float rn[3];   // record normal (towards the interior)
     float R;
     float uref;
     float cs, sn;  // 2D: cos/sin theta.  3D: cos theta, sqrt(1 - cos^2)
     float cph, sph;
-    float pd[3], pd2[3];
+    float pd[3];   // first tangent
     float gsum;
     int which;
 };
 
 template <int D>
+__device__ __forceinline__ void nd_centre(const NdState &st, float *c) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) c[k] = fmaf(st.rn[k], st.R, st.p[k]);
+}
+
+template <int D>
 __device__ __forceinline__ void nd_setup(NdState &st, const SceneView &S, const WalkCfg &c, const AdjCfg &a,
                                          uint32_t pt, uint32_t wk) {
     const uint4 rx = philox(c.rng, pt, wk, 0, ROLE_EXTRA);
-#pragma unroll
-    for (int k = 0; k < D; ++k) st.c[k] = fmaf(-st.n[k], st.R, st.p[k]);
     if (D == 2) {
         const float cu = a.clamping * wosm::kInv2Pi;
         const float u = fminf(fmaxf(wosm::u01(rx.x), cu), 1.0f - cu);
         wosm::sincos_2pi(u, &st.sn, &st.cs);
-        st.pd[0] = -st.n[1];
-        st.pd[1] = st.n[0];
+        st.pd[0] = st.rn[1];
+        st.pd[1] = -st.rn[0];
     } else {
         st.cs = fminf(fmaxf(fmaf(-2.0f, wosm::u01(rx.x), 1.0f), -1.0f), 1.0f - a.clamping);
         wosm::sincos_2pi(wosm::u01(rx.y), &st.sph, &st.cph);
-        const bool zu = fabsf(st.n[2]) < 0.9f;
+        const float n[3] = {-st.rn[0], -st.rn[1], -st.rn[2]};
+        const bool zu = fabsf(n[2]) < 0.9f;
         const float up0 = zu ? 0.0f : 1.0f, up2 = zu ? 1.0f : 0.0f;
-        cross3(st.n[0], st.n[1], st.n[2], up0, 0.0f, up2, st.pd[0], st.pd[1], st.pd[2]);
+        cross3(n[0], n[1], n[2], up0, 0.0f, up2, st.pd[0], st.pd[1], st.pd[2]);
         const float l = sqrtf(dot3(st.pd[0], st.pd[1], st.pd[2], st.pd[0], st.pd[1], st.pd[2]));
         for (int k = 0; k < 3; ++k) st.pd[k] = st.pd[k] / l;
-        cross3(st.n[0], st.n[1], st.n[2], st.pd[0], st.pd[1], st.pd[2], st.pd2[0], st.pd2[1], st.pd2[2]);
         st.sn = sqrtf(fmaxf(0.0f, fmaf(-st.cs, st.cs, 1.0f)));
     }
     st.gsum = 0.0f;
@@ -576,16 +582,21 @@ __device__ __forceinline__ void nd_setup(NdState &st, const SceneView &S, const 
 // Query point of antithetic sample st.which.
 template <int D>
 __device__ __forceinline__ void nd_point(const NdState &st, float *q) {
+    float c[3];
+    nd_centre<D>(st, c);
     if (D == 2) {
         const float si = st.which == 0 ? st.sn : -st.sn;
 #pragma unroll
-        for (int k = 0; k < 2; ++k) q[k] = fmaf(st.R, fmaf(st.n[k], st.cs, st.pd[k] * si), st.c[k]);
+        for (int k = 0; k < 2; ++k) q[k] = fmaf(st.R, fmaf(-st.rn[k], st.cs, st.pd[k] * si), c[k]);
         q[2] = 0.0f;
     } else {
+        const float n[3] = {-st.rn[0], -st.rn[1], -st.rn[2]};
+        float pd2[3];
+        cross3(n[0], n[1], n[2], st.pd[0], st.pd[1], st.pd[2], pd2[0], pd2[1], pd2[2]);
         const float cp = st.which == 0 ? st.cph : -st.cph, sp = st.which == 0 ? st.sph : -st.sph;
 #pragma unroll
         for (int k = 0; k < 3; ++k)
-            q[k] = fmaf(st.R, fmaf(st.cs, st.n[k], st.sn * fmaf(cp, st.pd[k], sp * st.pd2[k])), st.c[k]);
+            q[k] = fmaf(st.R, fmaf(st.cs, n[k], st.sn * fmaf(cp, st.pd[k], sp * pd2[k])), c[k]);
     }
 }
 
@@ -607,13 +618,15 @@ __device__ __forceinline__ void nd_finish(const NdState &st, const SceneView &S,
                                           uint32_t pt, uint32_t wk, bool with_src, float *out) {
     float grad = st.gsum * 0.5f;
     if (D == 2 && with_src) {
+        float ctr[3];
+        nd_centre<D>(st, ctr);
         const uint4 rx = philox(c.rng, pt, wk, 0, ROLE_EXTRA);
         float ds, dc;
         wosm::sincos_2pi(wosm::u01(rx.w), &ds, &dc);
         const float rr = sqrtf(wosm::u01(rx.z));
-        const float y[2] = {fmaf(st.R, rr * dc, st.c[0]), fmaf(st.R, rr * ds, st.c[1])};
+        const float y[2] = {fmaf(st.R, rr * dc, ctr[0]), fmaf(st.R, rr * ds, ctr[1])};
         const float f = source(S, y[0], y[1], nullptr);
-        const float P = eval_P(st.c, y, st.p, st.R);
+        const float P = eval_P(ctr, y, st.p, st.R);
         const float area = wosm::kPi * st.R * st.R;
         float ci;
         if (a.control_variates) {
@@ -625,7 +638,7 @@ __device__ __forceinline__ void nd_finish(const NdState &st, const SceneView &S,
         grad = grad - ci;
     }
 #pragma unroll
-    for (int k = 0; k < D; ++k) out[k] = grad * st.n[k];
+    for (int k = 0; k < D; ++k) out[k] = grad * -st.rn[k];
 }
 
 // Lane-local part of one inscribed-ball bisection step at radius m, centre q:
@@ -656,18 +669,37 @@ __device__ __forceinline__ void ball_precheck(const SceneView &S, const float *q
 enum { PH_IDLE = 0, PH_PRIMAL = 1, PH_BALL = 2, PH_ANTI_START = 3, PH_ANTI_WALK = 4, PH_ND_START = 5 };
 
 // Per-thread adjoint state kept in shared memory: touched at phase changes,
-// not in the query loop, so it does not occupy registers.
+// not in the query loop, so it does not occupy registers.  Only 4-byte
+// fields, an odd number of them: thread t's slot starts t * ADJ_SLOT_WORDS
+// words in, so a warp reading one field touches 32 distinct banks.
 struct AdjSlot {
     NdState st;
-    float rn[3];  // record normal (towards the interior)
     float rt0, rt1;
     float ba, bb;  // bisection bracket
     int bk;
     int bwarm;     // primitive that blocked the last rejected radius, or -1
     float tacc;    // tangent mode: the sample's directional derivative so far
-    double acc[5];  // source-parameter gradient accumulators
 };
-constexpr int ADJ_THREAD_WORDS = (int)((sizeof(AdjSlot) + 7) / 8);
+constexpr int ADJ_SLOT_WORDS = (int)(sizeof(AdjSlot) / 4) | 1;
+static_assert(sizeof(AdjSlot) % 4 == 0 && alignof(AdjSlot) == 4, "AdjSlot holds 4-byte fields only");
+
+// Shared memory after the guide table: [5 source-gradient accumulators x
+// blockDim doubles, field-major (when `acc`)][blockDim AdjSlot of
+// ADJ_SLOT_WORDS words].  Bytes per thread, for the launch's size.
+__host__ __device__ constexpr int adj_thread_bytes(bool acc) { return ADJ_SLOT_WORDS * 4 + (acc ? 40 : 0); }
+
+struct AdjSmem {
+    double *acc;  // this thread's first accumulator; the k-th is acc[k * blockDim.x]
+    AdjSlot *slot;
+};
+
+__device__ __forceinline__ AdjSmem adj_smem(double *base, bool acc) {
+    AdjSmem m;
+    m.acc = acc ? base + threadIdx.x : nullptr;
+    float *slots = reinterpret_cast<float *>(base + (acc ? 5 * blockDim.x : 0));
+    m.slot = reinterpret_cast<AdjSlot *>(slots + (size_t)threadIdx.x * ADJ_SLOT_WORDS);
+    return m;
+}
 
 // The adjoint kernel runs at most 256 threads per block and is compiled for
 // at least ADJ_MIN_BLOCKS resident blocks per SM: a 64-register cap.  The 3D
@@ -687,24 +719,28 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
                                                 unsigned long long *counter, int chunk, int n_top, int stage_cdf,
                                                 AdjOut out) {
     extern __shared__ float4 smem[];
-    const Smem sm = stage_smem(S, stage_cdf != 0, ADJ_THREAD_WORDS, smem);
+    const Smem sm = stage_smem(S, stage_cdf != 0, 0, smem);
     const unsigned short *cdf = sm.guide;
-    AdjSlot &slot = *reinterpret_cast<AdjSlot *>(sm.scratch);
-    double *acc_src = slot.acc;
+    const bool src2 = D == 2 && S.src_type != 0;
+    constexpr bool ND_ONLY = MODE == ADJ_ND_ONLY;
+    const bool want_src = !ND_ONLY && a.want_dsrc && c.include_source && src2;
+    const AdjSmem am = adj_smem(sm.scratch, want_src);
+    AdjSlot &slot = *am.slot;
+    double *acc_src = am.acc;  // k-th accumulator at acc_src[k * blockDim.x]
+    const int AS = blockDim.x;
+    if (want_src) {
 #pragma unroll
-    for (int k = 0; k < 5; ++k) acc_src[k] = 0.0;
+        for (int k = 0; k < 5; ++k) acc_src[k * AS] = 0.0;
+    }
     NdState &st = slot.st;
-    float *rn = slot.rn;
+    float *rn = st.rn;
     float &rt0 = slot.rt0, &rt1 = slot.rt1;
     float &ba = slot.ba, &bb = slot.bb;
     int &bk = slot.bk;
     int &bwarm = slot.bwarm;
-    const bool src2 = D == 2 && S.src_type != 0;
-    constexpr bool ND_ONLY = MODE == ADJ_ND_ONLY;
     constexpr bool TAN = MODE == ADJ_TANGENT;
     constexpr bool FROM_REC = MODE == ADJ_FROM_RECORDS || TAN;
     float &tacc = slot.tacc;
-    const bool want_src = !ND_ONLY && a.want_dsrc && c.include_source && src2;
     const bool with_src = a.source_in_nd && src2;
     Queue q{0, 0, false};
     bool active = false;
@@ -793,7 +829,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
                             if (want_src) {
 #pragma unroll
                                 for (int k = 0; k < 5; ++k)
-                                    acc_src[k] += W * (double)__ldg(&out.wds[(size_t)idx * 5 + k]);
+                                    acc_src[k * AS] += W * (double)__ldg(&out.wds[(size_t)idx * 5 + k]);
                             }
                         }
                         if (!a.want_dV || (TAN && out.tV == nullptr)) {
@@ -865,7 +901,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
             }
             if (want_src) {
 #pragma unroll
-                for (int k = 0; k < 5; ++k) acc_src[k] += W * (double)w.ds[k];
+                for (int k = 0; k < 5; ++k) acc_src[k * AS] += W * (double)w.ds[k];
             }
             if (!a.want_dV) {
                 active = false;
@@ -903,9 +939,6 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
                 continue;
             }
             st.R = ba;
-#pragma unroll
-            for (int k = 0; k < D; ++k) st.n[k] = -rn[k];
-            if (D == 2) st.n[2] = 0.0f;
             nd_setup<D>(st, S, c, a, pt, wk);
             nd_point<D>(st, qpos);
             phase = PH_ANTI_START;
@@ -986,7 +1019,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
     if (want_src && !TAN) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
-            double v = acc_src[k];
+            double v = acc_src[k * AS];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
             if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&out.dsrc[k], v);
@@ -1249,7 +1282,8 @@ static int launch_adjoint_t(const SceneImpl &S, const float *P, long long total,
     const WalkCfg c = make_cfg(p);
     const bool want_cdf = D == 2 && S.src_type != 0 && p.use_IS_for_greens;
     Shape sh;
-    int rc = shape_for(k_adjoint<D, BVH, ND>, S, D, BVH, want_cdf, sh, ADJ_THREAD_WORDS, 256);
+    const bool want_acc = ND != ADJ_ND_ONLY && a.want_dsrc && p.include_source && S.src_type != 0 && D == 2;
+    int rc = shape_for(k_adjoint<D, BVH, ND>, S, D, BVH, want_cdf, sh, (adj_thread_bytes(want_acc) + 7) / 8, 256);
     if (rc) return rc;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
@@ -1482,13 +1516,15 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
     unsigned long long *counter, int chunk, const int *__restrict__ wrec, const float *__restrict__ wds, double *acc,
     int count_work) {
     extern __shared__ float4 smem[];
-    AdjSlot &slot = *reinterpret_cast<AdjSlot *>(reinterpret_cast<double *>(smem) + (size_t)threadIdx.x * ADJ_THREAD_WORDS);
-    double *acc_src = slot.acc;
+    const AdjSmem am = adj_smem(reinterpret_cast<double *>(smem), true);
+    AdjSlot &slot = *am.slot;
+    double *acc_src = am.acc;  // k-th accumulator at acc_src[k * blockDim.x]
+    const int AS = blockDim.x;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) acc_src[k] = 0.0;
+    for (int k = 0; k < 5; ++k) acc_src[k * AS] = 0.0;
     int acc_item = -1;  // item whose source gradient acc_src holds
     NdState &st = slot.st;
-    float *rn = slot.rn;
+    float *rn = st.rn;
     float &rt0 = slot.rt0, &rt1 = slot.rt1;
     float &ba = slot.ba, &bb = slot.bb;
     int &bk = slot.bk;
@@ -1547,14 +1583,15 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
                         if (acc_item >= 0) {
 #pragma unroll
                             for (int k = 0; k < 5; ++k)
-                                if (acc_src[k] != 0.0) atomicAdd(&acc[items[acc_item].ds_off + k], acc_src[k]);
+                                if (acc_src[k * AS] != 0.0)
+                                    atomicAdd(&acc[items[acc_item].ds_off + k], acc_src[k * AS]);
                         }
 #pragma unroll
-                        for (int k = 0; k < 5; ++k) acc_src[k] = 0.0;
+                        for (int k = 0; k < 5; ++k) acc_src[k * AS] = 0.0;
                         acc_item = item;
                     }
 #pragma unroll
-                    for (int k = 0; k < 5; ++k) acc_src[k] += W * (double)__ldg(&wds[(size_t)idx * 5 + k]);
+                    for (int k = 0; k < 5; ++k) acc_src[k * AS] += W * (double)__ldg(&wds[(size_t)idx * 5 + k]);
                 }
                 if (!a.want_dV) {
                     active = false;
@@ -1609,9 +1646,6 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
                 continue;
             }
             st.R = ba;
-#pragma unroll
-            for (int k = 0; k < D; ++k) st.n[k] = -rn[k];
-            if (D == 2) st.n[2] = 0.0f;
             nd_setup<D>(st, S, c, a, pt, wk);
             nd_point<D>(st, qpos);
             phase = PH_ANTI_START;
@@ -1677,7 +1711,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
     if (acc_item >= 0) {
 #pragma unroll
         for (int k = 0; k < 5; ++k)
-            if (acc_src[k] != 0.0) atomicAdd(&acc[items[acc_item].ds_off + k], acc_src[k]);
+            if (acc_src[k * AS] != 0.0) atomicAdd(&acc[items[acc_item].ds_off + k], acc_src[k * AS]);
     }
 }
 
@@ -1730,7 +1764,7 @@ int launch_adjoint_batch(int D, const SceneView *views, const WalkCfg *cfgs, con
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
     const int block = std::min(L.block, 256);
-    const size_t smem = (size_t)block * ADJ_THREAD_WORDS * 8;
+    const size_t smem = (size_t)block * adj_thread_bytes(true) + 16;
     const int chunk = std::max(1, L.chunk / 2);
     int grid = 0;
     if (D == 2) {
