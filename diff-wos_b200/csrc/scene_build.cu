@@ -835,9 +835,12 @@ SceneView SceneImpl::view() const {
     v.tri = tri;
     v.nNodes = nNodes;
     v.node = node;
-    v.lseg = lseg;
-    v.lseginv = lseginv;
-    v.ltri = ltri;
+    // In input order the leaf-ordered copies equal the primitive arrays: point
+    // the kernels at one copy so the tree's leaf tests and the warm-start /
+    // record lookups share cache lines.
+    v.lseg = prim_order == 1 ? seg : lseg;
+    v.lseginv = prim_order == 1 ? seginv : lseginv;
+    v.ltri = prim_order == 1 ? tri : ltri;
     v.lorig = lorig;
     for (int k = 0; k < 3; ++k) {
         v.lo[k] = lo[k];

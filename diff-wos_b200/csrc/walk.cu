@@ -536,29 +536,35 @@ __device__ __forceinline__ float eval_P(const float *c, const float *y, const fl
 // outward normal n = -rn, the centre and the second tangent are recomputed
 // where needed (the same float operations as storing them), which keeps the
 // per-thread state small.
-struct NdState {
-    float p[3];    // boundary point
-    float rn[3];   // record normal (towards the interior)
+template <int D>
+struct NdExtra {};
+template <>
+struct NdExtra<3> {
+    float cph, sph;  // cos / sin of the azimuth
+};
+template <int D>
+struct NdState : NdExtra<D> {
+    float p[D];   // boundary point
+    float rn[D];  // record normal (towards the interior)
     float R;
     float uref;
     float cs, sn;  // 2D: cos/sin theta.  3D: cos theta, sqrt(1 - cos^2)
-    float cph, sph;
-    float pd[3];   // first tangent
+    float pd[D];   // first tangent
     float gsum;
     int which;
 };
 
 template <int D>
-__device__ __forceinline__ void nd_centre(const NdState &st, float *c) {
+__device__ __forceinline__ void nd_centre(const NdState<D> &st, float *c) {
 #pragma unroll
     for (int k = 0; k < D; ++k) c[k] = fmaf(st.rn[k], st.R, st.p[k]);
 }
 
 template <int D>
-__device__ __forceinline__ void nd_setup(NdState &st, const SceneView &S, const WalkCfg &c, const AdjCfg &a,
+__device__ __forceinline__ void nd_setup(NdState<D> &st, const SceneView &S, const WalkCfg &c, const AdjCfg &a,
                                          uint32_t pt, uint32_t wk) {
     const uint4 rx = philox(c.rng, pt, wk, 0, ROLE_EXTRA);
-    if (D == 2) {
+    if constexpr (D == 2) {
         const float cu = a.clamping * wosm::kInv2Pi;
         const float u = fminf(fmaxf(wosm::u01(rx.x), cu), 1.0f - cu);
         wosm::sincos_2pi(u, &st.sn, &st.cs);
@@ -581,10 +587,10 @@ __device__ __forceinline__ void nd_setup(NdState &st, const SceneView &S, const 
 
 // Query point of antithetic sample st.which.
 template <int D>
-__device__ __forceinline__ void nd_point(const NdState &st, float *q) {
+__device__ __forceinline__ void nd_point(const NdState<D> &st, float *q) {
     float c[3];
     nd_centre<D>(st, c);
-    if (D == 2) {
+    if constexpr (D == 2) {
         const float si = st.which == 0 ? st.sn : -st.sn;
 #pragma unroll
         for (int k = 0; k < 2; ++k) q[k] = fmaf(st.R, fmaf(-st.rn[k], st.cs, st.pd[k] * si), c[k]);
@@ -601,7 +607,7 @@ __device__ __forceinline__ void nd_point(const NdState &st, float *q) {
 }
 
 template <int D>
-__device__ __forceinline__ void nd_accumulate(NdState &st, const AdjCfg &a, float uq) {
+__device__ __forceinline__ void nd_accumulate(NdState<D> &st, const AdjCfg &a, float uq) {
     float P;
     if (D == 2) {
         P = 1.0f / (st.cs - 1.0f);
@@ -614,28 +620,30 @@ __device__ __forceinline__ void nd_accumulate(NdState &st, const AdjCfg &a, floa
 
 // grad * n_out, including the 2D interior source term.
 template <int D>
-__device__ __forceinline__ void nd_finish(const NdState &st, const SceneView &S, const WalkCfg &c, const AdjCfg &a,
-                                          uint32_t pt, uint32_t wk, bool with_src, float *out) {
+__device__ __forceinline__ void nd_finish(const NdState<D> &st, const SceneView &S, const WalkCfg &c,
+                                          const AdjCfg &a, uint32_t pt, uint32_t wk, bool with_src, float *out) {
     float grad = st.gsum * 0.5f;
-    if (D == 2 && with_src) {
-        float ctr[3];
-        nd_centre<D>(st, ctr);
-        const uint4 rx = philox(c.rng, pt, wk, 0, ROLE_EXTRA);
-        float ds, dc;
-        wosm::sincos_2pi(wosm::u01(rx.w), &ds, &dc);
-        const float rr = sqrtf(wosm::u01(rx.z));
-        const float y[2] = {fmaf(st.R, rr * dc, ctr[0]), fmaf(st.R, rr * ds, ctr[1])};
-        const float f = source(S, y[0], y[1], nullptr);
-        const float P = eval_P(ctr, y, st.p, st.R);
-        const float area = wosm::kPi * st.R * st.R;
-        float ci;
-        if (a.control_variates) {
-            const float fs = source(S, st.p[0], st.p[1], nullptr);
-            ci = (f - fs) * P * area + fs * st.R * 0.5f;
-        } else {
-            ci = f * P * area;
+    if constexpr (D == 2) {
+        if (with_src) {
+            float ctr[3];
+            nd_centre<D>(st, ctr);
+            const uint4 rx = philox(c.rng, pt, wk, 0, ROLE_EXTRA);
+            float ds, dc;
+            wosm::sincos_2pi(wosm::u01(rx.w), &ds, &dc);
+            const float rr = sqrtf(wosm::u01(rx.z));
+            const float y[2] = {fmaf(st.R, rr * dc, ctr[0]), fmaf(st.R, rr * ds, ctr[1])};
+            const float f = source(S, y[0], y[1], nullptr);
+            const float P = eval_P(ctr, y, st.p, st.R);
+            const float area = wosm::kPi * st.R * st.R;
+            float ci;
+            if (a.control_variates) {
+                const float fs = source(S, st.p[0], st.p[1], nullptr);
+                ci = (f - fs) * P * area + fs * st.R * 0.5f;
+            } else {
+                ci = f * P * area;
+            }
+            grad = grad - ci;
         }
-        grad = grad - ci;
     }
 #pragma unroll
     for (int k = 0; k < D; ++k) out[k] = grad * -st.rn[k];
@@ -672,32 +680,43 @@ enum { PH_IDLE = 0, PH_PRIMAL = 1, PH_BALL = 2, PH_ANTI_START = 3, PH_ANTI_WALK 
 // not in the query loop, so it does not occupy registers.  Only 4-byte
 // fields, an odd number of them: thread t's slot starts t * ADJ_SLOT_WORDS
 // words in, so a warp reading one field touches 32 distinct banks.
+template <int D>
 struct AdjSlot {
-    NdState st;
+    NdState<D> st;
     float rt0, rt1;
     float ba, bb;  // bisection bracket
     int bk;
     int bwarm;     // primitive that blocked the last rejected radius, or -1
     float tacc;    // tangent mode: the sample's directional derivative so far
 };
-constexpr int ADJ_SLOT_WORDS = (int)(sizeof(AdjSlot) / 4) | 1;
-static_assert(sizeof(AdjSlot) % 4 == 0 && alignof(AdjSlot) == 4, "AdjSlot holds 4-byte fields only");
+template <int D>
+constexpr int adj_slot_words() {
+    return (int)(sizeof(AdjSlot<D>) / 4) | 1;
+}
+static_assert(sizeof(AdjSlot<2>) % 4 == 0 && alignof(AdjSlot<2>) == 4 && sizeof(AdjSlot<3>) % 4 == 0 &&
+                  alignof(AdjSlot<3>) == 4,
+              "AdjSlot holds 4-byte fields only");
 
 // Shared memory after the guide table: [5 source-gradient accumulators x
 // blockDim doubles, field-major (when `acc`)][blockDim AdjSlot of
-// ADJ_SLOT_WORDS words].  Bytes per thread, for the launch's size.
-__host__ __device__ constexpr int adj_thread_bytes(bool acc) { return ADJ_SLOT_WORDS * 4 + (acc ? 40 : 0); }
+// adj_slot_words words].  Bytes per thread, for the launch's size.
+template <int D>
+__host__ __device__ constexpr int adj_thread_bytes(bool acc) {
+    return adj_slot_words<D>() * 4 + (acc ? 40 : 0);
+}
 
+template <int D>
 struct AdjSmem {
     double *acc;  // this thread's first accumulator; the k-th is acc[k * blockDim.x]
-    AdjSlot *slot;
+    AdjSlot<D> *slot;
 };
 
-__device__ __forceinline__ AdjSmem adj_smem(double *base, bool acc) {
-    AdjSmem m;
+template <int D>
+__device__ __forceinline__ AdjSmem<D> adj_smem(double *base, bool acc) {
+    AdjSmem<D> m;
     m.acc = acc ? base + threadIdx.x : nullptr;
     float *slots = reinterpret_cast<float *>(base + (acc ? 5 * blockDim.x : 0));
-    m.slot = reinterpret_cast<AdjSlot *>(slots + (size_t)threadIdx.x * ADJ_SLOT_WORDS);
+    m.slot = reinterpret_cast<AdjSlot<D> *>(slots + (size_t)threadIdx.x * adj_slot_words<D>());
     return m;
 }
 
@@ -724,15 +743,15 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
     const bool src2 = D == 2 && S.src_type != 0;
     constexpr bool ND_ONLY = MODE == ADJ_ND_ONLY;
     const bool want_src = !ND_ONLY && a.want_dsrc && c.include_source && src2;
-    const AdjSmem am = adj_smem(sm.scratch, want_src);
-    AdjSlot &slot = *am.slot;
+    const AdjSmem<D> am = adj_smem<D>(sm.scratch, want_src);
+    AdjSlot<D> &slot = *am.slot;
     double *acc_src = am.acc;  // k-th accumulator at acc_src[k * blockDim.x]
     const int AS = blockDim.x;
     if (want_src) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) acc_src[k * AS] = 0.0;
     }
-    NdState &st = slot.st;
+    NdState<D> &st = slot.st;
     float *rn = st.rn;
     float &rt0 = slot.rt0, &rt1 = slot.rt1;
     float &ba = slot.ba, &bb = slot.bb;
@@ -1283,7 +1302,7 @@ static int launch_adjoint_t(const SceneImpl &S, const float *P, long long total,
     const bool want_cdf = D == 2 && S.src_type != 0 && p.use_IS_for_greens;
     Shape sh;
     const bool want_acc = ND != ADJ_ND_ONLY && a.want_dsrc && p.include_source && S.src_type != 0 && D == 2;
-    int rc = shape_for(k_adjoint<D, BVH, ND>, S, D, BVH, want_cdf, sh, (adj_thread_bytes(want_acc) + 7) / 8, 256);
+    int rc = shape_for(k_adjoint<D, BVH, ND>, S, D, BVH, want_cdf, sh, (adj_thread_bytes<D>(want_acc) + 7) / 8, 256);
     if (rc) return rc;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
@@ -1516,14 +1535,14 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
     unsigned long long *counter, int chunk, const int *__restrict__ wrec, const float *__restrict__ wds, double *acc,
     int count_work) {
     extern __shared__ float4 smem[];
-    const AdjSmem am = adj_smem(reinterpret_cast<double *>(smem), true);
-    AdjSlot &slot = *am.slot;
+    const AdjSmem<D> am = adj_smem<D>(reinterpret_cast<double *>(smem), true);
+    AdjSlot<D> &slot = *am.slot;
     double *acc_src = am.acc;  // k-th accumulator at acc_src[k * blockDim.x]
     const int AS = blockDim.x;
 #pragma unroll
     for (int k = 0; k < 5; ++k) acc_src[k * AS] = 0.0;
     int acc_item = -1;  // item whose source gradient acc_src holds
-    NdState &st = slot.st;
+    NdState<D> &st = slot.st;
     float *rn = st.rn;
     float &rt0 = slot.rt0, &rt1 = slot.rt1;
     float &ba = slot.ba, &bb = slot.bb;
@@ -1764,7 +1783,7 @@ int launch_adjoint_batch(int D, const SceneView *views, const WalkCfg *cfgs, con
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
     const int block = std::min(L.block, 256);
-    const size_t smem = (size_t)block * adj_thread_bytes(true) + 16;
+    const size_t smem = (size_t)block * (D == 2 ? adj_thread_bytes<2>(true) : adj_thread_bytes<3>(true)) + 16;
     const int chunk = std::max(1, L.chunk / 2);
     int grid = 0;
     if (D == 2) {
