@@ -79,7 +79,7 @@ __device__ __forceinline__ void flush_work(const Work &wk) {
 // ball of radius ball_m centred at x (wball): it gets that primitive, or
 // prim = -1 when none blocks.  Brute force runs per lane and always returns
 // the nearest primitive.  Must be called by all 32 lanes.
-template <int D, bool BVH>
+template <int D, bool BVH, int WL = 0>
 __device__ __forceinline__ Hit warp_queries(const SceneView &S, bool active, const float *x, int warm, Work &work,
                                             float ball_m = -1.0f) {
     Hit mine{-1, INFINITY};
@@ -101,13 +101,13 @@ __device__ __forceinline__ Hit warp_queries(const SceneView &S, bool active, con
         const float bm = __shfl_sync(FULL, ball_m, j);
         Hit h{-1, INFINITY};
         if (bm > 0.0f) {
-            wball<D>(S, q, bm, h, work);
+            wball<D, WL>(S, q, bm, h, work);
         } else {
             if (wp >= 0) {
                 h.prim = wp;
                 h.d2 = prim_d2<D>(S, wp, q);
             }
-            h = wquery<D>(S, q, h, work);
+            h = wquery<D, WL>(S, q, h, work);
         }
         if (lane == j) mine = h;
     }
@@ -269,7 +269,7 @@ __device__ __forceinline__ bool refill(Queue &q, bool &active, long long &idx, u
 }
 
 // ------------------------------------------------------------------ forward
-template <int D, bool BVH, bool RECORDS>
+template <int D, bool BVH, bool RECORDS, int WL>
 __global__ void __launch_bounds__(512) k_walk(SceneView S, WalkCfg c, const float *__restrict__ P, long long total,
                                              unsigned long long *counter, int chunk, int n_top, int stage_cdf,
                                              WalkOut out) {
@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(512) k_walk(SceneView S, WalkCfg c, const floa
             walk_origin<D>(c, P, pt, wk, x0);
             w.start(x0, D);
         }
-        const Hit hit = warp_queries<D, BVH>(S, active, w.p, w.last, work);
+        const Hit hit = warp_queries<D, BVH, WL>(S, active, w.p, w.last, work);
         if (!active) continue;
         w.last = hit.prim;
         const int r = walker_advance<D>(w, S, hit, c, c.eps, c.project != 0, c.prevent_fd != 0, pt, wk, ROLE_PRIMAL,
@@ -732,7 +732,7 @@ __device__ __forceinline__ AdjSmem<D> adj_smem(double *base, bool acc) {
 // kernel writes one normal-derivative estimate per record (the
 // wos_normal_derivative entry point); otherwise items are (point, walk)
 // samples and gradients are accumulated into dV / dg / dsrc.
-template <int D, bool BVH, int MODE>
+template <int D, bool BVH, int MODE, int WL>
 __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, WalkCfg c, AdjCfg a, const float *__restrict__ P,
                                                 long long total, const float *__restrict__ dLdu,
                                                 unsigned long long *counter, int chunk, int n_top, int stage_cdf,
@@ -893,7 +893,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
         float ball_m = -1.0f;
         Hit pre{-1, INFINITY};
         if (active && phase == PH_BALL) ball_precheck<D>(S, qpos, (ba + bb) * 0.5f, bwarm, rprim, need, ball_m, pre);
-        Hit hit = warp_queries<D, BVH>(S, need, x, walking ? w.last : rprim, work, ball_m);
+        Hit hit = warp_queries<D, BVH, WL>(S, need, x, walking ? w.last : rprim, work, ball_m);
         if (!active) continue;
         if (phase == PH_BALL && (!need || (ball_m > 0.0f && hit.prim < 0))) hit = pre;
         if (walking) w.last = hit.prim;
@@ -1180,7 +1180,11 @@ static int shape_for(Kern kern, const SceneImpl &S, int D, bool bvh, bool want_c
     return 0;
 }
 
-template <int D, bool BVH>
+// Tree depths with their own kernel instance; deeper trees use the
+// any-depth instance (WL = 0).
+constexpr int WT_SPECIALISED_LEVELS = 3;
+
+template <int D, bool BVH, int WL>
 static int launch_walk_t(const SceneImpl &S, const float *P, long long total, const wos_params &p, bool records,
                          const WalkOut &out, unsigned long long *counter, cudaStream_t st) {
     const SceneView v = S.view();
@@ -1189,19 +1193,19 @@ static int launch_walk_t(const SceneImpl &S, const float *P, long long total, co
     Shape sh;
     int rc;
     if (records)
-        rc = shape_for(k_walk<D, BVH, true>, S, D, BVH, want_cdf, sh);
+        rc = shape_for(k_walk<D, BVH, true, WL>, S, D, BVH, want_cdf, sh);
     else
-        rc = shape_for(k_walk<D, BVH, false>, S, D, BVH, want_cdf, sh);
+        rc = shape_for(k_walk<D, BVH, false, WL>, S, D, BVH, want_cdf, sh);
     if (rc) return rc;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
     const int chunk = g_cfg[D - 2].chunk;
     if (records)
-        k_walk<D, BVH, true><<<sh.grid, sh.block, sh.smem, st>>>(v, c, P, total, counter, chunk, sh.n_top,
-                                                                  sh.stage_cdf, out);
+        k_walk<D, BVH, true, WL><<<sh.grid, sh.block, sh.smem, st>>>(v, c, P, total, counter, chunk, sh.n_top,
+                                                                      sh.stage_cdf, out);
     else
-        k_walk<D, BVH, false><<<sh.grid, sh.block, sh.smem, st>>>(v, c, P, total, counter, chunk, sh.n_top,
-                                                                   sh.stage_cdf, out);
+        k_walk<D, BVH, false, WL><<<sh.grid, sh.block, sh.smem, st>>>(v, c, P, total, counter, chunk, sh.n_top,
+                                                                       sh.stage_cdf, out);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail_cuda(e, "k_walk launch");
     return 0;
@@ -1211,11 +1215,20 @@ int launch_walk(const SceneImpl &S, const float *P, long long total, const wos_p
                 const WalkOut &out, unsigned long long *counter, cudaStream_t st) {
     if (total == 0) return 0;
     const bool bvh = p.use_bvh != 0;
-    if (S.dim == 2)
-        return bvh ? launch_walk_t<2, true>(S, P, total, p, records, out, counter, st)
-                   : launch_walk_t<2, false>(S, P, total, p, records, out, counter, st);
-    return bvh ? launch_walk_t<3, true>(S, P, total, p, records, out, counter, st)
-               : launch_walk_t<3, false>(S, P, total, p, records, out, counter, st);
+    const int wl = S.wt_levels <= WT_SPECIALISED_LEVELS ? S.wt_levels : 0;
+#define WOS_WALK(D_)                                                                        \
+    if (!bvh) return launch_walk_t<D_, false, 0>(S, P, total, p, records, out, counter, st); \
+    switch (wl) {                                                                           \
+        case 1: return launch_walk_t<D_, true, 1>(S, P, total, p, records, out, counter, st); \
+        case 2: return launch_walk_t<D_, true, 2>(S, P, total, p, records, out, counter, st); \
+        case 3: return launch_walk_t<D_, true, 3>(S, P, total, p, records, out, counter, st); \
+        default: return launch_walk_t<D_, true, 0>(S, P, total, p, records, out, counter, st); \
+    }
+    if (S.dim == 2) {
+        WOS_WALK(2)
+    }
+    WOS_WALK(3)
+#undef WOS_WALK
 }
 
 int launch_walk_plain(const SceneImpl &S, const float *P, long long total, const wos_params &p, float *values,
@@ -1293,7 +1306,7 @@ int launch_ball(const SceneImpl &S, const uint8_t *valid, const float *pt, const
     return 0;
 }
 
-template <int D, bool BVH, int ND>
+template <int D, bool BVH, int ND, int WL>
 static int launch_adjoint_t(const SceneImpl &S, const float *P, long long total, const wos_params &p,
                             const AdjCfg &a, const float *dLdu, const AdjOut &out, unsigned long long *counter,
                             cudaStream_t st) {
@@ -1302,13 +1315,14 @@ static int launch_adjoint_t(const SceneImpl &S, const float *P, long long total,
     const bool want_cdf = D == 2 && S.src_type != 0 && p.use_IS_for_greens;
     Shape sh;
     const bool want_acc = ND != ADJ_ND_ONLY && a.want_dsrc && p.include_source && S.src_type != 0 && D == 2;
-    int rc = shape_for(k_adjoint<D, BVH, ND>, S, D, BVH, want_cdf, sh, (adj_thread_bytes<D>(want_acc) + 7) / 8, 256);
+    int rc = shape_for(k_adjoint<D, BVH, ND, WL>, S, D, BVH, want_cdf, sh, (adj_thread_bytes<D>(want_acc) + 7) / 8,
+                       256);
     if (rc) return rc;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
     const int chunk = std::max(1, g_cfg[D - 2].chunk / 2);
-    k_adjoint<D, BVH, ND><<<sh.grid, sh.block, sh.smem, st>>>(v, c, a, P, total, dLdu, counter, chunk, sh.n_top,
-                                                              sh.stage_cdf, out);
+    k_adjoint<D, BVH, ND, WL><<<sh.grid, sh.block, sh.smem, st>>>(v, c, a, P, total, dLdu, counter, chunk, sh.n_top,
+                                                                  sh.stage_cdf, out);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail_cuda(e, "k_adjoint launch");
     return 0;
@@ -1318,20 +1332,30 @@ int launch_adjoint(const SceneImpl &S, const float *P, long long total, const wo
                    const float *dLdu, int mode, const AdjOut &out, unsigned long long *counter, cudaStream_t st) {
     if (total == 0) return 0;
     const bool bvh = p.use_bvh != 0;
-#define WOS_ADJ(D_, B_)                                                                                       \
-    switch (mode) {                                                                                           \
-        case ADJ_ND_ONLY: return launch_adjoint_t<D_, B_, ADJ_ND_ONLY>(S, P, total, p, a, dLdu, out, counter, st); \
-        case ADJ_FROM_RECORDS:                                                                                \
-            return launch_adjoint_t<D_, B_, ADJ_FROM_RECORDS>(S, P, total, p, a, dLdu, out, counter, st);     \
-        case ADJ_TANGENT: return launch_adjoint_t<D_, B_, ADJ_TANGENT>(S, P, total, p, a, dLdu, out, counter, st); \
-        default: return launch_adjoint_t<D_, B_, ADJ_RECOMPUTE>(S, P, total, p, a, dLdu, out, counter, st);  \
+    const int wl = S.wt_levels <= WT_SPECIALISED_LEVELS ? S.wt_levels : 0;
+#define WOS_ADJ_M(D_, B_, W_)                                                                                   \
+    switch (mode) {                                                                                             \
+        case ADJ_ND_ONLY: return launch_adjoint_t<D_, B_, ADJ_ND_ONLY, W_>(S, P, total, p, a, dLdu, out, counter, st); \
+        case ADJ_FROM_RECORDS:                                                                                  \
+            return launch_adjoint_t<D_, B_, ADJ_FROM_RECORDS, W_>(S, P, total, p, a, dLdu, out, counter, st);     \
+        case ADJ_TANGENT: return launch_adjoint_t<D_, B_, ADJ_TANGENT, W_>(S, P, total, p, a, dLdu, out, counter, st); \
+        default: return launch_adjoint_t<D_, B_, ADJ_RECOMPUTE, W_>(S, P, total, p, a, dLdu, out, counter, st);  \
+    }
+#define WOS_ADJ(D_)                          \
+    if (!bvh) {                              \
+        WOS_ADJ_M(D_, false, 0)              \
+    }                                        \
+    switch (wl) {                            \
+        case 1: WOS_ADJ_M(D_, true, 1)       \
+        case 2: WOS_ADJ_M(D_, true, 2)       \
+        case 3: WOS_ADJ_M(D_, true, 3)       \
+        default: WOS_ADJ_M(D_, true, 0)      \
     }
     if (S.dim == 2) {
-        if (bvh) WOS_ADJ(2, true);
-        WOS_ADJ(2, false);
+        WOS_ADJ(2)
     }
-    if (bvh) WOS_ADJ(3, true);
-    WOS_ADJ(3, false);
+    WOS_ADJ(3)
+#undef WOS_ADJ_M
 #undef WOS_ADJ
 }
 

@@ -607,10 +607,16 @@ __device__ __forceinline__ void wdescend(const SceneView &S, const float *q, int
     }
 }
 
-template <int D>
+// WL > 0: the tree has exactly WL levels (a kernel compiled for one depth
+// holds one descent, which keeps its code small); WL = 0: any depth.
+template <int D, int WL = 0>
 __device__ __forceinline__ Hit wquery(const SceneView &S, const float *q, Hit best, Work &wk) {
     const float tol2 = prune_tol2<D>(S, q);
     wk.nq += 1;
+    if constexpr (WL > 0) {
+        wdescend<D, WL>(S, q, 0, tol2, best, wk);
+        return best;
+    }
     switch (S.wt_levels) {
         case 1: wdescend<D, 1>(S, q, 0, tol2, best, wk); break;
         case 2: wdescend<D, 2>(S, q, 0, tol2, best, wk); break;
@@ -671,10 +677,11 @@ __device__ __forceinline__ bool wball_descend(const SceneView &S, const float *q
 // at q: returns true with a blocking primitive in `hit`, or false when no
 // primitive blocks.  Boxes are pruned against m^2 with the nearest search's
 // conservative tolerance, so no blocking primitive is missed.
-template <int D>
+template <int D, int WL = 0>
 __device__ __forceinline__ bool wball(const SceneView &S, const float *q, float m, Hit &hit, Work &wk) {
     const float bound = wt_bound((m * m) * (1.0f + 0x1p-20f), prune_tol2<D>(S, q));
     wk.nq += 1;
+    if constexpr (WL > 0) return wball_descend<D, WL>(S, q, 0, bound, m, hit, wk);
     switch (S.wt_levels) {
         case 1: return wball_descend<D, 1>(S, q, 0, bound, m, hit, wk);
         case 2: return wball_descend<D, 2>(S, q, 0, bound, m, hit, wk);
