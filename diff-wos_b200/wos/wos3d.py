@@ -26,6 +26,12 @@ class WoS3D(Solver):
         out = scene._native.normal_derivative(its.as_dict(), st, a)
         return out[:, 0], out[:, 1], out[:, 2]
 
+    def grad(self, p, scene, sampler):
+        """One finite-shell estimate of grad u per point (wos/wos3d.py:66-95):
+        two antithetic walks from the first ball with a control variate."""
+        from .gradient import finite_shell_grad
+        return finite_shell_grad(self, p, scene, sampler, with_source=False)
+
     def tangent_derivative(self, its, scene, sampler=None):
         return scene.tangent_derivative(its)
 

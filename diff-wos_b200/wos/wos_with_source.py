@@ -32,6 +32,13 @@ class WoSWithSource(WoS):
         self.G_cdf = np.cumsum(pmf) / pmf.sum()
         self.step = 1.0 / N
 
+    def grad(self, p, scene, sampler):
+        """One finite-shell estimate of grad u per point
+        (wos/wos_with_source.py:109-152): two antithetic walks from the
+        first ball with a control variate, plus the interior source term."""
+        from .gradient import finite_shell_grad
+        return finite_shell_grad(self, p, scene, sampler, with_source=True)
+
     def eval_G(self, p, R, r_clamp=1e-4):
         """Green's function of the disk of radius R at distance |p| from its centre."""
         r = torch.linalg.norm(p, dim=-1)
