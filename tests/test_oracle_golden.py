@@ -158,3 +158,16 @@ def test_oracle_lbvh_structure(oracle):
     assert sorted(internal.tolist()) == list(range(1, n - 1))
     assert sorted(leaves.tolist()) == list(range(n))
     assert np.all(np.diff(keys.astype(np.uint64)) > 0)
+
+
+def test_oracle_walk_from_a_nan_point_is_invalid(oracle):
+    """A point with no primitive at a finite distance ends as an invalid walk
+    (the kernels follow the same rule)."""
+    import numpy as np
+    from wos import shapes
+    V, F = shapes.circle(64)
+    S = oracle.OracleScene(V, F, np.ones(len(V), np.float32))
+    P = np.array([[np.nan, 0.0], [0.0, 0.0]], np.float32)
+    vals, valid, _ = S.walk_values(P, oracle.make_params(nwalks=2, nsteps=16, double_sided=True))
+    assert not valid[0].any() and (vals[0] == 0).all()
+    assert valid[1].all()
