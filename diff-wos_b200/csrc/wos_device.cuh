@@ -482,6 +482,19 @@ __device__ __forceinline__ float warp_min(float v) {
 }
 __device__ __forceinline__ int warp_min_int(int v) { return __reduce_min_sync(0xffffffffu, v); }
 
+// Frontier key of a lane: its child's distance with the low 5 mantissa bits
+// replaced by the lane, so one redux.sync minimum gives both the nearest
+// child and its lane.  The distance read back from a key (low bits cleared)
+// is at most the true one, so pruning on it stays conservative; only the
+// order of near-equal children (within 32 ulps) changes.
+__device__ __forceinline__ unsigned frontier_key(float d, int lane) {
+    return (__float_as_uint(d) & ~31u) | (unsigned)lane;
+}
+__device__ __forceinline__ float key_dist(unsigned k) { return __uint_as_float(k & ~31u); }
+// A taken entry: the largest +inf key (a NaN pattern would never compare
+// above the bound, so the loop could not end).
+constexpr unsigned KEY_TAKEN = 0x7f80001fu;
+
 template <int D>
 __device__ __forceinline__ float wt_box_d2(const SceneView &S, int node, const float *q) {
     float lo[3], hi[3];
@@ -578,12 +591,13 @@ __device__ __forceinline__ void wdescend(const SceneView &S, const float *q, int
     const int child = first + lane;
     float d = INFINITY;
     if (child < S.wt_count[L]) d = L == 1 ? leaf_bound<D>(S, child, q) : wt_box_d2<D>(S, S.wt_off[L] + child, q);
+    unsigned key = frontier_key(d, lane);
     wk.nb += 1;
     for (;;) {
-        const float m = warp_min(d);
-        if (m > wt_bound(best.d2, tol2)) return;
-        const int j = __ffs(__ballot_sync(FULL, d == m)) - 1;
-        if (lane == j) d = INFINITY;
+        const unsigned mk = __reduce_min_sync(FULL, key);
+        if (key_dist(mk) > wt_bound(best.d2, tol2)) return;
+        const int j = (int)(mk & 31u);
+        if (lane == j) key = KEY_TAKEN;
         const int node = first + j;
         if constexpr (L == 1) {
             wk.np += 1;
@@ -646,12 +660,13 @@ __device__ __forceinline__ bool wball_descend(const SceneView &S, const float *q
     const int child = first + lane;
     float d = INFINITY;
     if (child < S.wt_count[L]) d = L == 1 ? leaf_bound<D>(S, child, q) : wt_box_d2<D>(S, S.wt_off[L] + child, q);
+    unsigned key = frontier_key(d, lane);
     wk.nb += 1;
     for (;;) {
-        const float mn = warp_min(d);
-        if (mn > bound) return false;
-        const int j = __ffs(__ballot_sync(FULL, d == mn)) - 1;
-        if (lane == j) d = INFINITY;
+        const unsigned mk = __reduce_min_sync(FULL, key);
+        if (key_dist(mk) > bound) return false;
+        const int j = (int)(mk & 31u);
+        if (lane == j) key = KEY_TAKEN;
         const int node = first + j;
         if constexpr (L == 1) {
             wk.np += 1;
