@@ -457,6 +457,16 @@ def c3_main(args):
     b.record()
     torch.cuda.synchronize()
     t_plain = a.elapsed_time(b) * 1e-3
+    # tree work of one forward solve and one fused step (device counters, untimed)
+    wos.set_work_counting(True)
+    wos.work_counters(reset=True)
+    scene.solve(P, ws(1))
+    torch.cuda.synchronize()
+    fwd_work = wos.work_counters(reset=True)
+    scene.solve_adjoint(P, ws(1), adj, loss_kind=1)
+    torch.cuda.synchronize()
+    fused_work = wos.work_counters(reset=True)
+    wos.set_work_counting(False)
     walks = npts * nw
     line = {
         "metric": "wos_walks_per_s", "value": walks * args.steps / t, "unit": "walks/s", "n_gpus": 1,
@@ -469,6 +479,8 @@ def c3_main(args):
         "adjoint_pts_per_s": npts * args.steps / t,
         "forward_walks_per_s": walks / t_fwd,
         "plain_forward_walks_per_s": m * nw / t_plain,
+        "tree_work": {"forward": fwd_work, "forward_and_adjoint": fused_work,
+                      "note": "queries, node expansions, leaf steps (one warp step each)"},
         "accuracy": {"rmse_vs_exact": float(np.sqrt((err ** 2).mean())), "rms_standard_error":
                      float(np.sqrt((se ** 2).mean())),
                      "truncated_fraction": float((steps.cpu().numpy() >= 64).mean())},
