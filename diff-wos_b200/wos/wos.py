@@ -43,6 +43,12 @@ class WoS(Solver):
     def tangent_derivative(self, its, scene, sampler=None):
         return scene.tangent_derivative(its)
 
+    def grad(self, p, scene, sampler):
+        """One finite-shell estimate of grad u per point (the estimator of
+        wos/wos_with_source.py:109-152 without its source term)."""
+        from .gradient import finite_shell_grad
+        return finite_shell_grad(self, p, scene, sampler, with_source=False)
+
 
 @dataclass
 class WoSCUDA(WoS):
