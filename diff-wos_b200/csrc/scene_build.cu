@@ -847,6 +847,12 @@ SceneView SceneImpl::view() const {
         v.hi[k] = hi[k];
     }
     v.half_min_extent = half_min_extent;
+    v.max_extent = 0.0f;
+    for (int k = 0; k < dim; ++k) {
+        v.max_extent = fmaxf(v.max_extent, hi[k] - lo[k]);
+        v.centre[k] = (lo[k] + hi[k]) * 0.5f;
+    }
+    for (int k = dim; k < 3; ++k) v.centre[k] = 0.0f;
     v.src_type = src_type;
     for (int k = 0; k < 5; ++k) v.src[k] = src[k];
     v.cdf = cdf;

@@ -53,6 +53,8 @@ struct SceneView {
     const int *lorig;
     float lo[3], hi[3];
     float half_min_extent;  // min_k (hi_k - lo_k) / 2
+    float max_extent;       // max_k (hi_k - lo_k)
+    float centre[3];        // (lo + hi) / 2
     int src_type;
     float src[5];
     const float *cdf;  // G CDF table (n_cdf entries)
@@ -298,11 +300,9 @@ struct Work {
 // bounds the coordinates' magnitude around the scene.
 template <int D>
 __device__ __forceinline__ float prune_tol2(const SceneView &S, const float *p) {
-    float s = 0.0f;
+    float s = S.max_extent;
 #pragma unroll
-    for (int k = 0; k < D; ++k) s = fmaxf(s, S.hi[k] - S.lo[k]);
-#pragma unroll
-    for (int k = 0; k < D; ++k) s += fabsf(p[k] - (S.lo[k] + S.hi[k]) * 0.5f);
+    for (int k = 0; k < D; ++k) s += fabsf(p[k] - S.centre[k]);
     const float e = s * 9.5367431640625e-07f;
     return 1025.0f * (e * e);
 }
