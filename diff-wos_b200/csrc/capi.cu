@@ -564,6 +564,42 @@ int wos_solve_tangent(wos_scene_t scene, const float *P, int n, const wos_params
     return launch_reduce(tan, n, p->nwalks, tangent, tangent_var, st);
 }
 
+size_t wos_soft_walk_workspace_size(int n, const wos_params *p) {
+    if (p == nullptr || n < 0 || p->nwalks < 1) return 0;
+    const size_t nw = (size_t)n * (size_t)p->nwalks;
+    return 256 + 2 * align256(sizeof(float) * nw);
+}
+
+int wos_soft_walk(wos_scene_t scene, const float *P, int n, const wos_params *p, const float *dV_dir,
+                  const float *dg_dir, double *mean, double *var, double *tangent, double *tangent_var, void *workspace,
+                  size_t workspace_bytes, wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (int rc = check_params(p)) return rc;
+    if (p->nsteps < 1) return fail(WOS_ERR_INVALID_ARGUMENT, "the soft-edge walk needs nsteps >= 1");
+    if (!(p->epsilon > 0.0f)) return fail(WOS_ERR_INVALID_ARGUMENT, "the soft-edge walk needs epsilon > 0");
+    if (n < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "n must be >= 0");
+    if (n == 0) return 0;
+    WOS_CHECK_DEV(P, "P");
+    WOS_CHECK_DEV(mean, "mean");
+    WOS_CHECK_DEV_OPT(var, "var");
+    WOS_CHECK_DEV_OPT(tangent, "tangent");
+    WOS_CHECK_DEV_OPT(tangent_var, "tangent_var");
+    WOS_CHECK_DEV_OPT(dV_dir, "dV_dir");
+    WOS_CHECK_DEV_OPT(dg_dir, "dg_dir");
+    cudaStream_t st = (cudaStream_t)stream;
+    Scratch s;
+    if (int rc = s.init(workspace, workspace_bytes, wos_soft_walk_workspace_size(n, p), st)) return rc;
+    const size_t nw = (size_t)n * (size_t)p->nwalks;
+    unsigned long long *counter = (unsigned long long *)s.base;
+    float *vals = (float *)(s.base + 256);
+    float *tans = tangent != nullptr ? (float *)(s.base + 256 + align256(sizeof(float) * nw)) : nullptr;
+    if (int rc = launch_walk_soft(scene->impl, P, (long long)nw, *p, dV_dir, dg_dir, vals, tans, counter, st))
+        return rc;
+    if (int rc = launch_reduce(vals, n, p->nwalks, mean, var, st)) return rc;
+    if (tans != nullptr) return launch_reduce(tans, n, p->nwalks, tangent, tangent_var, st);
+    return 0;
+}
+
 int wos_boundary_term(wos_scene_t scene, const wos_detector *det, int nwalks, uint64_t seed, const float *dV_dir,
                       double *image_tangent, const float *dLdI, float *dV, wos_stream_t stream) {
     if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");

@@ -1231,6 +1231,260 @@ int launch_walk(const SceneImpl &S, const float *P, long long total, const wos_p
 #undef WOS_WALK
 }
 
+// ------------------------------------------------------------------ soft-edge walk
+// The soft-edge walk of the reference's Baseline / Baseline3D
+// (wos/wos.py:158-187, wos/wos_grad_3d.py:24-57): nsteps steps, each adding
+// beta (1 - w) g(closest point) with w = min(d, eps) / eps and then
+// beta *= w; it never stops early.  Forward mode carries the tangents of the
+// position, the distance, beta and the result along a vertex / value motion.
+
+// Barycentric region of the closest point on a triangle, by the cascade of
+// tri_closest: 0 vertex a, 1 b, 2 c, 3 edge ab, 4 ac, 5 bc, 6 face, 7 degenerate.
+__device__ __forceinline__ int tri_region(float4 t0, float4 t1, float4 t2, const float *x) {
+    const float axx = x[0] - t0.x, axy = x[1] - t0.y, axz = x[2] - t0.z;
+    const float ab2 = t0.w, abac = t1.w, ac2 = t2.w;
+    const float d1 = dot3(t1.x, t1.y, t1.z, axx, axy, axz);
+    const float d2 = dot3(t2.x, t2.y, t2.z, axx, axy, axz);
+    if (d1 <= 0.0f && d2 <= 0.0f) return 0;
+    const float d3 = d1 - ab2, d4 = d2 - abac;
+    if (d3 >= 0.0f && d4 <= d3) return 1;
+    const float d5 = d1 - abac, d6 = d2 - ac2;
+    if (d6 >= 0.0f && d5 <= d6) return 2;
+    const float vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) return 3;
+    const float vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) return 4;
+    const float va = d3 * d6 - d5 * d4;
+    if (va <= 0.0f && d4 - d3 >= 0.0f && d5 - d6 >= 0.0f) return 5;
+    return va + vb + vc > 0.0f ? 6 : 7;
+}
+
+// Derivative of the projection parameter t = (x - a).e / (e.e) of x onto
+// the line a + t e, for motions xd, ad, ed.
+__device__ __forceinline__ float proj_dot(const float *x, const float *a, const float *e, const float *xd,
+                                          const float *ad, const float *ed, int D, float t) {
+    float ee = 0.0f, num = 0.0f, eed = 0.0f;
+    for (int k = 0; k < D; ++k) {
+        ee += e[k] * e[k];
+        num += (xd[k] - ad[k]) * e[k] + (x[k] - a[k]) * ed[k];
+        eed += e[k] * ed[k];
+    }
+    return ee > 0.0f ? (num - 2.0f * t * eed) / ee : 0.0f;
+}
+
+// Tangents at a soft-walk step: of the nearest distance d (> 0) to primitive
+// prim at x, dd = n.(xd - cd) with n = (x - c)/d and cd the motion of the
+// closest point at fixed barycentrics (n is normal to the feature, so the
+// barycentrics' own motion drops out); and of the boundary value there, gd
+// (barycentric motion through the projection plus value motion).  tV / tg:
+// vertex and value directions, either may be null.
+template <int D>
+__device__ void soft_tangents(const SceneView &S, const float *x, const float *xd, float d, const Rec &r, int prim,
+                              const float *tV, const float *tg, float &dd, float &gd) {
+    int vid[3];
+    float wts[3];
+    dirichlet<D>(S, prim, r.t0, r.t1, vid, wts);
+    float V[3][3], Vd[3][3];
+    for (int j = 0; j < D; ++j)
+        for (int k = 0; k < 3; ++k) {
+            V[j][k] = k < D ? __ldg(&S.V[(size_t)vid[j] * D + k]) : 0.0f;
+            Vd[j][k] = (tV != nullptr && k < D) ? __ldg(&tV[(size_t)vid[j] * D + k]) : 0.0f;
+        }
+    float cd[3] = {0.0f, 0.0f, 0.0f};
+    for (int j = 0; j < D; ++j)
+        for (int k = 0; k < D; ++k) cd[k] = fmaf(wts[j], Vd[j][k], cd[k]);
+    dd = 0.0f;
+    if (d > 0.0f)
+        for (int k = 0; k < D; ++k) dd += (x[k] - r.p[k]) / d * (xd[k] - cd[k]);
+    // barycentric motion
+    float bd[3] = {0.0f, 0.0f, 0.0f};  // d(wts)/dt
+    if (D == 2) {
+        if (r.t0 > 0.0f && r.t0 < 1.0f) {
+            const float e[2] = {V[1][0] - V[0][0], V[1][1] - V[0][1]};
+            const float ed[2] = {Vd[1][0] - Vd[0][0], Vd[1][1] - Vd[0][1]};
+            const float td = proj_dot(x, V[0], e, xd, Vd[0], ed, 2, r.t0);
+            bd[0] = -td;
+            bd[1] = td;
+        }
+    } else {
+        const float4 t0 = __ldg(&S.tri[3 * prim]), t1 = __ldg(&S.tri[3 * prim + 1]), t2 = __ldg(&S.tri[3 * prim + 2]);
+        const int reg = tri_region(t0, t1, t2, x);
+        float ab[3], ac[3], abd[3], acd[3];
+        for (int k = 0; k < 3; ++k) {
+            ab[k] = V[1][k] - V[0][k];
+            ac[k] = V[2][k] - V[0][k];
+            abd[k] = Vd[1][k] - Vd[0][k];
+            acd[k] = Vd[2][k] - Vd[0][k];
+        }
+        if (reg == 3) {
+            const float vd = proj_dot(x, V[0], ab, xd, Vd[0], abd, 3, r.t0);
+            bd[1] = vd;
+            bd[0] = -vd;
+        } else if (reg == 4) {
+            const float wd = proj_dot(x, V[0], ac, xd, Vd[0], acd, 3, r.t1);
+            bd[2] = wd;
+            bd[0] = -wd;
+        } else if (reg == 5) {
+            float bc[3], bcd[3];
+            for (int k = 0; k < 3; ++k) {
+                bc[k] = V[2][k] - V[1][k];
+                bcd[k] = Vd[2][k] - Vd[1][k];
+            }
+            const float wd = proj_dot(x, V[1], bc, xd, Vd[1], bcd, 3, r.t1);
+            bd[2] = wd;
+            bd[1] = -wd;
+        } else if (reg == 6) {
+            // G [v w]^T = rhs: G = [[ab.ab, ab.ac], [ab.ac, ac.ac]], rhs = [ab.(x-a), ac.(x-a)]
+            float G00 = 0, G01 = 0, G11 = 0, Gd00 = 0, Gd01 = 0, Gd11 = 0, rd0 = 0, rd1 = 0;
+            for (int k = 0; k < 3; ++k) {
+                const float xa = x[k] - V[0][k], xad = xd[k] - Vd[0][k];
+                G00 += ab[k] * ab[k];
+                G01 += ab[k] * ac[k];
+                G11 += ac[k] * ac[k];
+                Gd00 += 2.0f * ab[k] * abd[k];
+                Gd01 += abd[k] * ac[k] + ab[k] * acd[k];
+                Gd11 += 2.0f * ac[k] * acd[k];
+                rd0 += abd[k] * xa + ab[k] * xad;
+                rd1 += acd[k] * xa + ac[k] * xad;
+            }
+            const float q0 = rd0 - (Gd00 * r.t0 + Gd01 * r.t1), q1 = rd1 - (Gd01 * r.t0 + Gd11 * r.t1);
+            const float det = G00 * G11 - G01 * G01;
+            if (det != 0.0f) {
+                const float vd = (G11 * q0 - G01 * q1) / det, wd = (G00 * q1 - G01 * q0) / det;
+                bd[1] = vd;
+                bd[2] = wd;
+                bd[0] = -vd - wd;
+            }
+        }
+    }
+    gd = 0.0f;
+    for (int j = 0; j < D; ++j) {
+        const float gj = __ldg(&S.g[vid[j]]);
+        gd = fmaf(bd[j], gj, gd);
+        if (tg != nullptr) gd = fmaf(wts[j], __ldg(&tg[vid[j]]), gd);
+    }
+}
+
+template <int D, bool BVH, int WL>
+__global__ void __launch_bounds__(256) k_walk_soft(SceneView S, WalkCfg c, const float *__restrict__ P,
+                                                   long long total, unsigned long long *counter, int chunk,
+                                                   const float *__restrict__ tV, const float *__restrict__ tg,
+                                                   float *vals, float *tans) {
+    Queue q{0, 0, false};
+    bool active = false;
+    long long idx = 0;
+    uint32_t pt = 0, wk = 0;
+    float p[3] = {0, 0, 0}, pd[3] = {0, 0, 0};
+    float beta = 0.0f, betad = 0.0f, res = 0.0f, resd = 0.0f;
+    int i = 0, last = -1;
+    bool fresh = false;
+    const float eps = c.eps;
+    const bool want_tan = tans != nullptr;
+    Work work{0, 0, 0};
+    for (;;) {
+        const bool was = active;
+        if (!refill(q, active, idx, counter, total, chunk)) break;
+        if (active && !was) {
+            pt = (uint32_t)(idx / c.nwalks);
+            wk = c.walk_offset + (uint32_t)(idx - (long long)pt * c.nwalks);
+            walk_origin<D>(c, P, pt, wk, p);
+            pd[0] = pd[1] = pd[2] = 0.0f;
+            beta = 1.0f;
+            betad = res = resd = 0.0f;
+            i = 0;
+            last = -1;
+            fresh = true;
+        }
+        const Hit hit = warp_queries<D, BVH, WL>(S, active, p, last, work);
+        if (!active) continue;
+        last = hit.prim;
+        bool done = hit.prim < 0;
+        if (!done && fresh) {
+            fresh = false;
+            if (!c.double_sided && !inside_test<D>(S, p, hit, nullptr)) done = true;
+        }
+        if (done) {
+            vals[idx] = 0.0f;
+            if (want_tan) tans[idx] = 0.0f;
+            active = false;
+            continue;
+        }
+        const float d = sqrtf(hit.d2);
+        const Rec r = closest_record<D>(S, p, hit.prim);
+        const float g = dirichlet<D>(S, hit.prim, r.t0, r.t1, nullptr, nullptr);
+        float dd = 0.0f, gd = 0.0f;
+        if (want_tan) soft_tangents<D>(S, p, pd, d, r, hit.prim, tV, tg, dd, gd);
+        const float w = fminf(d, eps) / eps;
+        const float wd = d < eps ? dd / eps : 0.0f;
+        if (d > 0.0f) {
+            res = fmaf(beta * (1.0f - w), g, res);
+            if (want_tan) resd += betad * (1.0f - w) * g - beta * wd * g + beta * (1.0f - w) * gd;
+        }
+        betad = betad * w + beta * wd;
+        beta = beta * w;
+        if (i >= c.nsteps - 1) {
+            vals[idx] = res;
+            if (want_tan) tans[idx] = resd;
+            active = false;
+            continue;
+        }
+        const uint4 rr = philox(c.rng, pt, wk, (uint32_t)i, ROLE_PRIMAL);
+        float dir[3];
+        if (D == 2) {
+            float s, cs;
+            wosm::sincos_2pi(wosm::u01(rr.x), &s, &cs);
+            dir[0] = cs;
+            dir[1] = s;
+            dir[2] = 0.0f;
+        } else {
+            const float z = fmaf(-2.0f, wosm::u01(rr.x), 1.0f);
+            const float rad = sqrtf(fmaxf(0.0f, fmaf(-z, z, 1.0f)));
+            float s, cs;
+            wosm::sincos_2pi(wosm::u01(rr.y), &s, &cs);
+            dir[0] = rad * cs;
+            dir[1] = rad * s;
+            dir[2] = z;
+        }
+        for (int k = 0; k < D; ++k) {
+            p[k] = fmaf(dir[k], d, p[k]);
+            pd[k] = fmaf(dir[k], dd, pd[k]);
+        }
+        ++i;
+    }
+    if (c.count) flush_work<BVH>(work);
+}
+
+template <int D, bool BVH, int WL>
+static int launch_soft_t(const SceneImpl &S, const float *P, long long total, const wos_params &p, const float *tV,
+                         const float *tg, float *vals, float *tans, unsigned long long *counter, cudaStream_t st) {
+    const SceneView v = S.view();
+    const WalkCfg c = make_cfg(p);
+    int grid = 0;
+    int dev = 0, sms = 148, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_walk_soft<D, BVH, WL>, 256, 0);
+    if (e != cudaSuccess) return fail_cuda(e, "occupancy(k_walk_soft)");
+    grid = std::max(1, per) * sms;
+    e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
+    k_walk_soft<D, BVH, WL><<<grid, 256, 0, st>>>(v, c, P, total, counter, 32, tV, tg, vals, tans);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_walk_soft launch");
+    return 0;
+}
+
+int launch_walk_soft(const SceneImpl &S, const float *P, long long total, const wos_params &p, const float *tV,
+                     const float *tg, float *vals, float *tans, unsigned long long *counter, cudaStream_t st) {
+    if (total == 0) return 0;
+    const bool bvh = p.use_bvh != 0;
+    if (S.dim == 2)
+        return bvh ? launch_soft_t<2, true, 0>(S, P, total, p, tV, tg, vals, tans, counter, st)
+                   : launch_soft_t<2, false, 0>(S, P, total, p, tV, tg, vals, tans, counter, st);
+    return bvh ? launch_soft_t<3, true, 0>(S, P, total, p, tV, tg, vals, tans, counter, st)
+               : launch_soft_t<3, false, 0>(S, P, total, p, tV, tg, vals, tans, counter, st);
+}
+
 int launch_walk_plain(const SceneImpl &S, const float *P, long long total, const wos_params &p, float *values,
                       cudaStream_t st) {
     if (total == 0) return 0;

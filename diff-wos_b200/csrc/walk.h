@@ -104,6 +104,9 @@ int get_launch_config(int dim, wos_launch_config *out);
 
 int launch_walk(const SceneImpl &S, const float *P, long long total, const wos_params &p, bool records,
                 const WalkOut &out, unsigned long long *counter, cudaStream_t st);
+// Soft-edge walk values (and, with tans, forward-mode tangents along tV / tg).
+int launch_walk_soft(const SceneImpl &S, const float *P, long long total, const wos_params &p, const float *tV,
+                     const float *tg, float *vals, float *tans, unsigned long long *counter, cudaStream_t st);
 int launch_walk_plain(const SceneImpl &S, const float *P, long long total, const wos_params &p, float *values,
                       cudaStream_t st);
 int launch_reduce(const float *vals, int n, int nw, double *mean, double *var, cudaStream_t st);

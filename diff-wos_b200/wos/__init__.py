@@ -16,7 +16,7 @@ from .stats import Statistics
 from .wos import Baseline, WoS, WoSCUDA
 from .wos3d import WoS3D, WoS3DCUDA
 from .wos_grad import Ours, OursCUDA
-from .wos_grad_3d import Ours3D
+from .wos_grad_3d import Baseline3D, Ours3D
 from .baselines import Baseline2, Baseline2CUDA, Baseline23D
 from .wos_boundary import WoSBoundary
 from .wos_with_source import WoSWithSource, WoSWithSourceCUDA
@@ -26,5 +26,5 @@ __all__ = [
     "Detector", "Detector3D", "Detector3DY", "Intersection", "Ours", "Ours3D", "OursCUDA", "Polyline", "Sampler",
     "Scene3D", "Solver", "Statistics", "WoS", "WoS3D", "WoS3DCUDA", "WoSCUDA", "WoSWithSource", "WoSWithSourceCUDA",
     "Baseline", "WosError", "device_status", "get_launch_config", "set_launch_config", "set_work_counting",
-    "work_counters", "shapes", "BatchItem", "BatchPlan", "WoSBoundary", "Baseline2", "Baseline2CUDA", "Baseline23D",
+    "work_counters", "shapes", "BatchItem", "BatchPlan", "WoSBoundary", "Baseline2", "Baseline2CUDA", "Baseline23D", "Baseline3D",
 ]

@@ -317,6 +317,26 @@ class NativeScene:
                  stream())
         return dict(mean=mean, var=var, tangent=tan, tangent_var=tvar)
 
+    def soft_walk(self, P, s: WalkSettings, dV=None, dg=None, want_tangent=False, want_var=False):
+        """Soft-edge walk (wos_soft_walk): per-point mean of the walk values
+        and, with want_tangent, of their derivatives along (dV, dg)."""
+        P = as_cuda(P, torch.float32, self.dim)
+        n = int(P.shape[0])
+        d = self.device
+        mean = torch.empty(n, dtype=torch.float64, device=d)
+        var = torch.empty(n, dtype=torch.float64, device=d) if want_var else None
+        tan = torch.empty(n, dtype=torch.float64, device=d) if want_tangent else None
+        tvar = torch.empty(n, dtype=torch.float64, device=d) if (want_tangent and want_var) else None
+        tV = as_cuda(dV, torch.float32, self.dim) if dV is not None else None
+        tg = as_cuda(dg, torch.float32).reshape(-1) if dg is not None else None
+        if n:
+            c = s.c()
+            need = _lib.lib().wos_soft_walk_workspace_size(n, ctypes.byref(c))
+            ws = torch.empty(need, dtype=torch.uint8, device=d)
+            call("wos_soft_walk", self.h, P.data_ptr(), n, ctypes.byref(c), _ptr(tV), _ptr(tg), mean.data_ptr(),
+                 _ptr(var), _ptr(tan), _ptr(tvar), ws.data_ptr(), need, stream())
+        return dict(mean=mean, var=var, tangent=tan, tangent_var=tvar)
+
     def boundary_term(self, det, nwalks: int, seed: int = 0, dV_dir=None, dLdI=None):
         """Image-space boundary term (wos_boundary_term): the derivative image
         for vertex motion dV_dir (forward mode) and / or the vertex gradient

@@ -58,13 +58,60 @@ class WoSCUDA(WoS):
     project_unterminated = False
 
 
+class _SoftFunction(torch.autograd.Function):
+    """Per-point means of the soft-edge walk, differentiable in forward mode
+    (the reference's renderD use of Baseline, diff_solve/runner.py:75-109)."""
+
+    @staticmethod
+    def forward(ctx, solver, scene, P, s, vertices, values):
+        ctx.solver, ctx.scene, ctx.P, ctx.s = solver, scene, P, s
+        return scene._native.soft_walk(P, s)["mean"].to(torch.float32)
+
+    @staticmethod
+    def jvp(ctx, _solver, _scene, _P, _s, dV, dg):
+        out = ctx.scene._native.soft_walk(ctx.P, ctx.s, dV=dV, dg=dg, want_tangent=True)
+        return out["tangent"].to(torch.float32)
+
+    @staticmethod
+    def backward(ctx, grad):
+        raise NotImplementedError("the soft-edge baseline is differentiated in forward mode only "
+                                  "(torch.autograd.forward_ad); use OursCUDA for reverse mode")
+
+
+class _SoftWalk:
+    """The soft-edge walk (wos/wos.py:158-187, wos/wos_grad_3d.py:24-57):
+    every walk takes nsteps steps, adding beta (1 - w) g with
+    w = min(d, epsilon) / epsilon and then beta *= w.  Values and their
+    forward-mode derivatives come from the wos_soft_walk kernel."""
+
+    def soft_settings(self, scene, seed, jitter=None):
+        from .native import WalkSettings
+        return WalkSettings(nwalks=int(self.nwalks), nsteps=int(self.nsteps), epsilon=float(self.epsilon),
+                            double_sided=bool(self.double_sided), use_bvh=bool(scene.use_bvh), seed=int(seed),
+                            jitter=tuple(jitter) if jitter is not None else (0.0, 0.0, 0.0))
+
+    def walk(self, p, scene, seed=0, jitter=None):
+        from .fwd import points
+        from .solver import has_tangent
+        P = points(p, scene.dim)
+        s = self.soft_settings(scene, seed, jitter)
+        V, g = scene.vertices, scene.values
+        if has_tangent(V) or has_tangent(g) or (torch.is_grad_enabled() and (V.requires_grad or g.requires_grad)):
+            return _SoftFunction.apply(self, scene, P, s, V, g)
+        return scene._native.soft_walk(P, s)["mean"].to(torch.float32)
+
+    def solve(self, p, scene, seed=0, jitter=None):
+        from .fwd import points
+        return scene._native.soft_walk(points(p, scene.dim), self.soft_settings(scene, seed, jitter))["mean"].to(
+            torch.float32)
+
+    def walk_detector(self, scene, detector, seed=0):
+        return self.walk(detector.make_points(), scene, seed, jitter=detector.jitter())
+
+
 @dataclass
-class Baseline(Solver):
-    """Soft-edge fully differentiated walk (wos/wos.py:158-187) is a
-    comparison estimator outside the hot path; not provided."""
+class Baseline(_SoftWalk, Solver):
+    """Soft-edge walk on polylines (wos/wos.py:158-187)."""
     epsilon: float = 0.005
     nwalks: int = 10
     nsteps: int = 32
-
-    def walk(self, p, scene, seed=0):
-        raise NotImplementedError("Baseline is not part of the B200 hot path")

@@ -3,6 +3,8 @@ from __future__ import annotations
 
 from dataclasses import dataclass
 
+from .solver import Solver
+from .wos import _SoftWalk
 from .wos_grad import OursCUDA
 
 
@@ -13,3 +15,11 @@ class Ours3D(OursCUDA):
     (wos/wos3d.py:288-307)."""
     epsilon2: float = 1e-3
     clamping: float = 1e-1
+
+
+@dataclass
+class Baseline3D(_SoftWalk, Solver):
+    """Soft-edge walk on triangle meshes (wos/wos_grad_3d.py:24-57)."""
+    epsilon: float = 0.005
+    nwalks: int = 10
+    nsteps: int = 32

@@ -290,6 +290,23 @@ WOS_API int wos_solve_tangent(wos_scene_t scene, const float *P, int n, const wo
                               const float *dsrc_dir, double *mean, double *var, double *tangent, double *tangent_var,
                               void *workspace, size_t workspace_bytes, wos_stream_t stream);
 
+/* Workspace of wos_soft_walk. */
+WOS_API size_t wos_soft_walk_workspace_size(int n, const wos_params *p);
+
+/* The soft-edge walk of the reference's Baseline / Baseline3D
+ * (wos/wos.py:158-187, wos/wos_grad_3d.py:24-57): every walk takes exactly
+ * p->nsteps steps (nsteps >= 1), each adding beta (1 - w) g(closest point)
+ * with w = min(d, epsilon) / epsilon, then beta *= w; p->epsilon is the
+ * soft-edge width.  mean / var: per-point mean and variance of the walk
+ * values.  Forward mode: when `tangent` is given, the per-point mean (and
+ * variance) of each walk's derivative along dV_dir (nV x dim) and dg_dir
+ * (nV), either may be NULL: the motion of every step's distance, weight,
+ * position and boundary value is carried through the walk (the reference
+ * differentiates the same walk with Dr.Jit). */
+WOS_API int wos_soft_walk(wos_scene_t scene, const float *P, int n, const wos_params *p, const float *dV_dir,
+                          const float *dg_dir, double *mean, double *var, double *tangent, double *tangent_var,
+                          void *workspace, size_t workspace_bytes, wos_stream_t stream);
+
 /* A detector: res[0] x res[1] pixels over [vmin, vmax] in scene axes
  * (axis_u, axis_v); in 3D a slab |x[slab_axis] - slab_center| <
  * slab_half_width (slab_axis -1 in 2D); size = its area (2D) or slab volume

@@ -105,6 +105,7 @@ def lib() -> ctypes.CDLL:
         L.orc_philox.argtypes = [ctypes.c_uint64, P, P, I]
         L.orc_tri_closest.argtypes = [P, P, P, P, I, P, P]
         L.orc_walk_counted.argtypes = [P, P, I, ctypes.POINTER(Params), P, I, P]
+        L.orc_soft_walk.argtypes = [P, P, I, ctypes.POINTER(Params), P, I]
         L.orc_adjoint_counted.argtypes = [P, P, I, ctypes.POINTER(Params), ctypes.POINTER(AdjParams), P, P, P, P, I,
                                           P]
         _lib = L
@@ -224,6 +225,14 @@ class OracleScene:
                           _p(dg), _p(ds), nthreads)
         return dV, dg, ds
 
+
+    def soft_walk(self, P, params: Params, nthreads=0):
+        """Per-walk values of the soft-edge walk (Baseline), points x walks."""
+        P = _f32(P)
+        n = P.shape[0]
+        vals = np.zeros((n, params.nwalks), np.float32)
+        lib().orc_soft_walk(self.h, _p(P), n, ctypes.byref(params), _p(vals), nthreads)
+        return vals
 
     def walk_counted(self, P, params: Params, nthreads=0):
         """Per-walk values plus LBVH work totals {queries, node visits, prims}."""

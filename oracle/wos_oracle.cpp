@@ -1146,6 +1146,67 @@ void orc_inscribed_ball(void *s, const float *pt, const float *nrm, const unsign
     }
 }
 
+// Soft-edge walk of Baseline / Baseline3D (wos/wos.py:158-187,
+// wos/wos_grad_3d.py:24-57): exactly nsteps steps, each adding
+// beta (1 - w) g with w = min(d, eps) / eps, then beta *= w.
+static float soft_walk(const Scene &S, const float *p0, const Params &prm, const Rng &rng, uint32_t pt, uint32_t wk) {
+    const int D = S.D;
+    const bool bvh = prm.use_bvh != 0;
+    float p[3] = {p0[0], p0[1], D == 3 ? p0[2] : 0.0f};
+    if (prm.jitter[0] != 0.0f || prm.jitter[1] != 0.0f || prm.jitter[2] != 0.0f) {
+        const U4 r = rng.draw(pt, wk, 0, ROLE_JITTER);
+        p[0] = fmaf(wosm::u01(r.x) - 0.5f, prm.jitter[0], p[0]);
+        p[1] = fmaf(wosm::u01(r.y) - 0.5f, prm.jitter[1], p[1]);
+        if (D == 3) p[2] = fmaf(wosm::u01(r.z) - 0.5f, prm.jitter[2], p[2]);
+    }
+    Hit hit = nearest(S, p, bvh);
+    if (hit.prim < 0) return 0.0f;
+    if (!prm.double_sided && !sdf_from_hit(S, p, hit).inside) return 0.0f;
+    const float eps = prm.epsilon;
+    float beta = 1.0f, res = 0.0f;
+    for (int i = 0; i < prm.nsteps; ++i) {
+        const float d = sqrtf(hit.d2);
+        const Rec r = closest_record(S, p, hit.prim);
+        const float g = dirichlet(S, r);
+        const float w = fminf(d, eps) / eps;
+        if (d > 0.0f) res = fmaf(beta * (1.0f - w), g, res);
+        beta = beta * w;
+        if (i == prm.nsteps - 1) break;
+        const U4 rr = rng.draw(pt, wk, (uint32_t)i, ROLE_PRIMAL);
+        float dir[3] = {0.0f, 0.0f, 0.0f};
+        if (D == 2) {
+            float s, c;
+            wosm::sincos_2pi(wosm::u01(rr.x), &s, &c);
+            dir[0] = c;
+            dir[1] = s;
+        } else {
+            const float z = fmaf(-2.0f, wosm::u01(rr.x), 1.0f);
+            const float rad = sqrtf(fmaxf(0.0f, fmaf(-z, z, 1.0f)));
+            float s, c;
+            wosm::sincos_2pi(wosm::u01(rr.y), &s, &c);
+            dir[0] = rad * c;
+            dir[1] = rad * s;
+            dir[2] = z;
+        }
+        for (int k = 0; k < D; ++k) p[k] = fmaf(dir[k], d, p[k]);
+        hit = nearest(S, p, bvh);
+        if (hit.prim < 0) return 0.0f;
+    }
+    return res;
+}
+
+void orc_soft_walk(void *s, const float *P, int n, const Params *prm, float *vals, int nthreads) {
+    Scene *S = (Scene *)s;
+    const Rng rng = make_rng(prm->seed);
+    const int nw = prm->nwalks;
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long t = 0; t < (long long)n * nw; ++t) {
+        const int i = (int)(t / nw), w = (int)(t % nw);
+        vals[t] = soft_walk(*S, &P[(size_t)i * S->D], *prm, rng, (uint32_t)i, prm->walk_offset + (uint32_t)w);
+    }
+}
+
 // Per-walk values for points x walks; vals[i * nwalks + w].
 void orc_walk_values(void *s, const float *P, int n, const Params *prm, float *vals, unsigned char *valid,
                      int *steps, int nthreads) {

@@ -162,3 +162,60 @@ def test_batched_scenes_ranges_and_seeding():
             assert sc["F"].shape[0] in (320, 1280)
         np.testing.assert_allclose(sc["g"], shapes.harmonic_poly(sc["V"], sc["coeffs"], sc["degree"]), rtol=1e-5,
                                    atol=1e-5)
+
+
+def test_soft_walk_tangent_formulas_float64():
+    """The forward-mode rules of the soft-edge walk (distance motion
+    n . (dx - dc) at fixed barycentrics, projection-parameter motion of the
+    boundary value, weight and throughput products), restated in float64
+    numpy on a brute-force polyline, agree with central differences away
+    from the |sdf| kink."""
+    from wos import shapes
+    V, F = shapes.star(96, 0.6, 0.2, 4)
+    V = V.astype(np.float64)
+    rng = np.random.default_rng(2)
+    g = V[:, 0] ** 2 - V[:, 1] ** 2 + 0.5 * V[:, 0]
+    dV = rng.normal(size=V.shape) * 0.2
+    dV[:, 0] += 1.0
+    dg = rng.normal(size=len(V))
+    eps = 5e-2
+
+    def nearest(Vv, x):
+        a, b = Vv[F[:, 0]], Vv[F[:, 1]]
+        e = b - a
+        t = np.clip(((x - a) * e).sum(1) / (e * e).sum(1), 0, 1)
+        c = a + t[:, None] * e
+        d2 = ((x - c) ** 2).sum(1)
+        j = int(np.argmin(d2))
+        return j, np.sqrt(d2[j]), t[j], c[j]
+
+    def walk(Vv, gv, x0, dirs, tan=False):
+        x, xd = x0.copy(), np.zeros(2)
+        beta, betad, res, resd = 1.0, 0.0, 0.0, 0.0
+        for om in dirs:
+            j, d, t, c = nearest(Vv, x)
+            ia, ib = F[j]
+            val = gv[ia] + t * (gv[ib] - gv[ia])
+            dd = vd = 0.0
+            if tan:
+                cd = (1 - t) * dV[ia] + t * dV[ib]
+                dd = (x - c) / d @ (xd - cd)
+                e, ed = Vv[ib] - Vv[ia], dV[ib] - dV[ia]
+                td = (((xd - dV[ia]) @ e + (x - Vv[ia]) @ ed) - 2 * t * (e @ ed)) / (e @ e) if 0 < t < 1 else 0.0
+                vd = td * (gv[ib] - gv[ia]) + (1 - t) * dg[ia] + t * dg[ib]
+            w = min(d, eps) / eps
+            wd = dd / eps if d < eps else 0.0
+            res += beta * (1 - w) * val
+            resd += betad * (1 - w) * val - beta * wd * val + beta * (1 - w) * vd
+            betad, beta = betad * w + beta * wd, beta * w
+            x, xd = x + d * om, xd + dd * om
+        return res, resd
+
+    h = 1e-6
+    for k in range(25):
+        th = rng.uniform(0, 2 * np.pi, 8)
+        dirs = np.stack([np.cos(th), np.sin(th)], 1)
+        x0 = rng.uniform(-0.3, 0.3, 2)
+        _, tan = walk(V, g, x0, dirs, tan=True)
+        fd = (walk(V + h * dV, g + h * dg, x0, dirs)[0] - walk(V - h * dV, g - h * dg, x0, dirs)[0]) / (2 * h)
+        assert abs(fd - tan) < 1e-4 * (1 + abs(tan)), (k, fd, tan)
