@@ -11,7 +11,7 @@ import os
 from pathlib import Path
 
 _HERE = Path(__file__).resolve().parent
-LIB_PATH = Path(os.environ.get("WOS_B200_LIB", _HERE.parent / "lib" / "libwos_b200.so"))
+LIB_PATH = Path(os.environ.get("WOS_B200_LIB") or _HERE.parent / "lib" / "libwos_b200.so")
 
 WOS_OK = 0
 WOS_ERR_INVALID_ARGUMENT = -1
