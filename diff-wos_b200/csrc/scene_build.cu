@@ -527,6 +527,87 @@ __global__ void k_wt_level(const float4 *in, int n_in, float4 *out, int n_out) {
     }
 }
 
+// Slab bounds of the level-2 nodes of a 3D wide tree (patches of up to 1024
+// triangles), the same construction as the leaves' in k_wt_level1: the
+// normalised sum of the unit face normals, and the interval of n.(v - c) over
+// the vertices, c the node's box centre, widened for rounding.  One block of
+// SLAB_THREADS per node; fixed-order reductions.  The half-thickness goes to
+// the box's first .w, the normal and the interval's centre to slab[node].
+constexpr int SLAB_THREADS = 256;
+__global__ void __launch_bounds__(SLAB_THREADS) k_wt_slab2(const float4 *ltri, int nF, float4 *box, float4 *slab,
+                                                            int n2) {
+    __shared__ double red[3][SLAB_THREADS];
+    const int i = blockIdx.x, t = threadIdx.x;
+    if (i >= n2) return;
+    const int b0 = WT_LEAF * 32 * i, e = min(b0 + WT_LEAF * 32, nF);
+    double ns[3] = {0.0, 0.0, 0.0};
+    for (int s = b0 + t; s < e; s += SLAB_THREADS) {
+        const float4 ab = ltri[3 * s + 1], ac = ltri[3 * s + 2];
+        double nn[3];
+        nn[0] = (double)ab.y * ac.z - (double)ab.z * ac.y;
+        nn[1] = (double)ab.z * ac.x - (double)ab.x * ac.z;
+        nn[2] = (double)ab.x * ac.y - (double)ab.y * ac.x;
+        const double l = sqrt(nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2]);
+        if (l > 0.0)
+            for (int k = 0; k < 3; ++k) ns[k] += nn[k] / l;
+    }
+    for (int k = 0; k < 3; ++k) red[k][t] = ns[k];
+    __syncthreads();
+    for (int h = SLAB_THREADS / 2; h > 0; h >>= 1) {
+        if (t < h)
+            for (int k = 0; k < 3; ++k) red[k][t] += red[k][t + h];
+        __syncthreads();
+    }
+    for (int k = 0; k < 3; ++k) ns[k] = red[k][0];
+    __syncthreads();
+    const float4 ba = box[2 * i], bb = box[2 * i + 1];
+    const float lo[3] = {ba.x, ba.y, ba.z}, hi[3] = {bb.x, bb.y, bb.z};
+    float c[3];
+    for (int k = 0; k < 3; ++k) c[k] = (lo[k] + hi[k]) * 0.5f;
+    const double ln = sqrt(ns[0] * ns[0] + ns[1] * ns[1] + ns[2] * ns[2]);
+    float nf[3] = {0.0f, 0.0f, 0.0f};
+    float ocf = 0.0f, ohf = INFINITY;
+    if (ln > 1e-6) {
+        // unit normal, shrunk by 2^-20 so that |n| <= 1 after rounding
+        for (int k = 0; k < 3; ++k) nf[k] = (float)(ns[k] / ln * (1.0 - 0x1p-20));
+        double omin = INFINITY, omax = -INFINITY, diag2 = 0.0;
+        for (int k = 0; k < 3; ++k) diag2 += ((double)hi[k] - lo[k]) * ((double)hi[k] - lo[k]);
+        for (int s = b0 + t; s < e; s += SLAB_THREADS) {
+            const float4 a = ltri[3 * s], ab = ltri[3 * s + 1], ac = ltri[3 * s + 2];
+            const double av[3] = {a.x, a.y, a.z}, abv[3] = {ab.x, ab.y, ab.z}, acv[3] = {ac.x, ac.y, ac.z};
+            for (int j = 0; j < 3; ++j) {
+                double o = 0.0;
+                for (int k = 0; k < 3; ++k) {
+                    const double v = av[k] + (j == 1 ? abv[k] : j == 2 ? acv[k] : 0.0);
+                    o += (double)nf[k] * (v - (double)c[k]);
+                }
+                omin = fmin(omin, o);
+                omax = fmax(omax, o);
+            }
+        }
+        red[0][t] = omin;
+        red[1][t] = omax;
+        __syncthreads();
+        for (int h = SLAB_THREADS / 2; h > 0; h >>= 1) {
+            if (t < h) {
+                red[0][t] = fmin(red[0][t], red[0][t + h]);
+                red[1][t] = fmax(red[1][t], red[1][t + h]);
+            }
+            __syncthreads();
+        }
+        omin = red[0][0];
+        omax = red[1][0];
+        const double oc = 0.5 * (omin + omax);
+        ocf = (float)oc;
+        const double oh = 0.5 * (omax - omin) + fabs(oc - (double)ocf) + 1e-6 * sqrt(diag2);
+        ohf = __double2float_ru(oh);
+    }
+    if (t == 0) {
+        box[2 * i].w = ohf;
+        slab[i] = make_float4(nf[0], nf[1], nf[2], ocf);
+    }
+}
+
 // ------------------------------------------------------------------ host
 static inline int nblk(long long n, int b) { return (int)((n + b - 1) / b); }
 
@@ -707,13 +788,17 @@ static int build_geometry(SceneImpl &S, cudaStream_t st) {
         WOS_TRY(dalloc(&S.wt_box, (size_t)off * W, st));
         if (S.wt_slab) cudaFreeAsync(S.wt_slab, st);
         S.wt_slab = nullptr;
-        WOS_TRY(dalloc(&S.wt_slab, (size_t)S.wt_count[1], st));
+        const bool slab2 = D == 3 && WOS_SLAB_LEVELS >= 2 && S.wt_levels >= 2;
+        WOS_TRY(dalloc(&S.wt_slab, (size_t)S.wt_count[1] + (slab2 ? S.wt_count[2] : 0), st));
         k_wt_level1<D><<<nblk(S.wt_count[1], TB), TB, 0, st>>>(skeys, nF, pbox, S.lseg, S.ltri, S.wt_box, S.wt_slab,
                                                                S.wt_count[1]);
         for (int l = 2; l <= S.wt_levels; ++l)
             k_wt_level<D><<<nblk(S.wt_count[l], TB), TB, 0, st>>>(S.wt_box + (size_t)S.wt_off[l - 1] * W,
                                                                 S.wt_count[l - 1], S.wt_box + (size_t)S.wt_off[l] * W,
                                                                 S.wt_count[l]);
+        if (slab2)
+            k_wt_slab2<<<S.wt_count[2], SLAB_THREADS, 0, st>>>(S.ltri, nF, S.wt_box + (size_t)S.wt_off[2] * W,
+                                                               S.wt_slab + S.wt_count[1], S.wt_count[2]);
         WOS_TRY(cudaGetLastError());
     }
 

@@ -516,18 +516,27 @@ __device__ __forceinline__ float wt_box_d2(const SceneView &S, int node, const f
     return box_d2<D>(lo, hi, q);
 }
 
-// Lower bound on the squared distance from q to leaf `leaf`: in 3D the
-// larger of its box distance and its slab distance; in 2D the box distance
-// (polyline pieces are thin enough in their boxes that the slab test costs
-// more than it prunes).
-template <int D>
-__device__ __forceinline__ float leaf_bound(const SceneView &S, int leaf, const float *q) {
+// 3D levels whose nodes carry a slab bound beside their box: the leaves and,
+// with WOS_SLAB_LEVELS 2, their parents (patches of 1024 triangles, whose box
+// is loose wherever the surface is tilted against the axes).
+#ifndef WOS_SLAB_LEVELS
+#define WOS_SLAB_LEVELS 2
+#endif
+
+// Lower bound on the squared distance from q to node `node` of level L: in 3D
+// (levels up to WOS_SLAB_LEVELS) the larger of its box distance and its slab
+// distance; otherwise, and in 2D, the box distance (polyline pieces are thin
+// enough in their boxes that the slab test costs more than it prunes).  The
+// slabs of level 2 follow those of level 1 in wt_slab.
+template <int D, int L>
+__device__ __forceinline__ float node_bound(const SceneView &S, int node, const float *q) {
     float lo[3], hi[3], n[3], c[3], oc, oh;
-    if (D == 2) {
-        return wt_box_d2<2>(S, S.wt_off[1] + leaf, q);
+    if (D == 2 || L > WOS_SLAB_LEVELS) {
+        return wt_box_d2<D>(S, S.wt_off[L] + node, q);
     } else {
-        const float4 a = __ldg(&S.wt_box[2 * (S.wt_off[1] + leaf)]), b = __ldg(&S.wt_box[2 * (S.wt_off[1] + leaf) + 1]);
-        const float4 sl = __ldg(&S.wt_slab[leaf]);
+        const int bi = S.wt_off[L] + node;
+        const float4 a = __ldg(&S.wt_box[2 * bi]), b = __ldg(&S.wt_box[2 * bi + 1]);
+        const float4 sl = __ldg(&S.wt_slab[L == 1 ? node : S.wt_count[1] + node]);
         lo[0] = a.x;
         lo[1] = a.y;
         lo[2] = a.z;
@@ -590,7 +599,7 @@ __device__ __forceinline__ void wdescend(const SceneView &S, const float *q, int
     const int lane = threadIdx.x & 31;
     const int child = first + lane;
     float d = INFINITY;
-    if (child < S.wt_count[L]) d = L == 1 ? leaf_bound<D>(S, child, q) : wt_box_d2<D>(S, S.wt_off[L] + child, q);
+    if (child < S.wt_count[L]) d = node_bound<D, L>(S, child, q);
     unsigned key = frontier_key(d, lane);
     wk.nb += 1;
     for (;;) {
@@ -659,7 +668,7 @@ __device__ __forceinline__ bool wball_descend(const SceneView &S, const float *q
     const int lane = threadIdx.x & 31;
     const int child = first + lane;
     float d = INFINITY;
-    if (child < S.wt_count[L]) d = L == 1 ? leaf_bound<D>(S, child, q) : wt_box_d2<D>(S, S.wt_off[L] + child, q);
+    if (child < S.wt_count[L]) d = node_bound<D, L>(S, child, q);
     unsigned key = frontier_key(d, lane);
     wk.nb += 1;
     for (;;) {
