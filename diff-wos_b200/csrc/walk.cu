@@ -202,11 +202,13 @@ __device__ __forceinline__ int walker_advance(Walker &w, const SceneView &S, con
     return project ? W_VALID : W_TRUNC;
 }
 
-// Dynamic shared memory: [G-CDF guide table][per-thread scratch of
-// `thread_words` 8-byte words].
-__host__ __device__ inline size_t smem_bytes(int n_guide, int nthreads, int thread_words) {
+// Dynamic shared memory: [G-CDF guide table][`thread_bytes` of scratch per
+// thread].  Sized to the byte: the carve-out the driver picks for the
+// kernel's resident blocks comes in steps, and every byte of it is L1 lost to
+// the tree.
+__host__ __device__ inline size_t smem_bytes(int n_guide, int nthreads, int thread_bytes) {
     size_t b = ((size_t)(n_guide + 1) * sizeof(unsigned short) + 15) & ~(size_t)15;
-    b += (size_t)nthreads * thread_words * 8;
+    b += ((size_t)nthreads * thread_bytes + 15) & ~(size_t)15;
     return b;
 }
 
@@ -541,6 +543,7 @@ struct NdExtra {};
 template <>
 struct NdExtra<3> {
     float cph, sph;  // cos / sin of the azimuth
+    float pd[3];     // first tangent (in 2D it is recomputed from the normal)
 };
 template <int D>
 struct NdState : NdExtra<D> {
@@ -549,7 +552,6 @@ struct NdState : NdExtra<D> {
     float R;
     float uref;
     float cs, sn;  // 2D: cos/sin theta.  3D: cos theta, sqrt(1 - cos^2)
-    float pd[D];   // first tangent
     float gsum;
     int which;
 };
@@ -560,6 +562,21 @@ __device__ __forceinline__ void nd_centre(const NdState<D> &st, float *c) {
     for (int k = 0; k < D; ++k) c[k] = fmaf(st.rn[k], st.R, st.p[k]);
 }
 
+// First tangent of the ball frame at the boundary point: in 2D the record
+// normal turned by a right angle, recomputed where it is used (a smaller
+// per-sample slot leaves more of the SM's L1 to the tree); in 3D stored by
+// nd_setup (recomputing it costs more than the L1 it frees).
+template <int D>
+__device__ __forceinline__ void nd_tangent(const NdState<D> &st, float *pd) {
+    if constexpr (D == 2) {
+        pd[0] = st.rn[1];
+        pd[1] = -st.rn[0];
+    } else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) pd[k] = st.pd[k];
+    }
+}
+
 template <int D>
 __device__ __forceinline__ void nd_setup(NdState<D> &st, const SceneView &S, const WalkCfg &c, const AdjCfg &a,
                                          uint32_t pt, uint32_t wk) {
@@ -568,8 +585,6 @@ __device__ __forceinline__ void nd_setup(NdState<D> &st, const SceneView &S, con
         const float cu = a.clamping * wosm::kInv2Pi;
         const float u = fminf(fmaxf(wosm::u01(rx.x), cu), 1.0f - cu);
         wosm::sincos_2pi(u, &st.sn, &st.cs);
-        st.pd[0] = st.rn[1];
-        st.pd[1] = -st.rn[0];
     } else {
         st.cs = fminf(fmaxf(fmaf(-2.0f, wosm::u01(rx.x), 1.0f), -1.0f), 1.0f - a.clamping);
         wosm::sincos_2pi(wosm::u01(rx.y), &st.sph, &st.cph);
@@ -588,21 +603,22 @@ __device__ __forceinline__ void nd_setup(NdState<D> &st, const SceneView &S, con
 // Query point of antithetic sample st.which.
 template <int D>
 __device__ __forceinline__ void nd_point(const NdState<D> &st, float *q) {
-    float c[3];
+    float c[3], pd[3];
     nd_centre<D>(st, c);
+    nd_tangent<D>(st, pd);
     if constexpr (D == 2) {
         const float si = st.which == 0 ? st.sn : -st.sn;
 #pragma unroll
-        for (int k = 0; k < 2; ++k) q[k] = fmaf(st.R, fmaf(-st.rn[k], st.cs, st.pd[k] * si), c[k]);
+        for (int k = 0; k < 2; ++k) q[k] = fmaf(st.R, fmaf(-st.rn[k], st.cs, pd[k] * si), c[k]);
         q[2] = 0.0f;
     } else {
         const float n[3] = {-st.rn[0], -st.rn[1], -st.rn[2]};
         float pd2[3];
-        cross3(n[0], n[1], n[2], st.pd[0], st.pd[1], st.pd[2], pd2[0], pd2[1], pd2[2]);
+        cross3(n[0], n[1], n[2], pd[0], pd[1], pd[2], pd2[0], pd2[1], pd2[2]);
         const float cp = st.which == 0 ? st.cph : -st.cph, sp = st.which == 0 ? st.sph : -st.sph;
 #pragma unroll
         for (int k = 0; k < 3; ++k)
-            q[k] = fmaf(st.R, fmaf(st.cs, n[k], st.sn * fmaf(cp, st.pd[k], sp * pd2[k])), c[k]);
+            q[k] = fmaf(st.R, fmaf(st.cs, n[k], st.sn * fmaf(cp, pd[k], sp * pd2[k])), c[k]);
     }
 }
 
@@ -1157,14 +1173,14 @@ struct Shape {
 
 template <typename Kern>
 static int shape_for(Kern kern, const SceneImpl &S, int D, bool bvh, bool want_cdf, Shape &sh,
-                     int thread_words = 0, int max_block = 512) {
+                     int thread_bytes = 0, int max_block = 512) {
     const wos_launch_config &cfg = g_cfg[D - 2];
     sh.block = std::min(cfg.block_threads, max_block);
     // the persistent kernels query the wide tree cooperatively; no binary-LBVH
     // nodes are staged
     sh.n_top = 0;
     sh.stage_cdf = want_cdf ? 1 : 0;
-    sh.smem = smem_bytes(want_cdf ? S.n_guide : -1, sh.block, thread_words);
+    sh.smem = smem_bytes(want_cdf ? S.n_guide : -1, sh.block, thread_bytes);
     (void)bvh;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
@@ -1569,8 +1585,7 @@ static int launch_adjoint_t(const SceneImpl &S, const float *P, long long total,
     const bool want_cdf = D == 2 && S.src_type != 0 && p.use_IS_for_greens;
     Shape sh;
     const bool want_acc = ND != ADJ_ND_ONLY && a.want_dsrc && p.include_source && S.src_type != 0 && D == 2;
-    int rc = shape_for(k_adjoint<D, BVH, ND, WL>, S, D, BVH, want_cdf, sh, (adj_thread_bytes<D>(want_acc) + 7) / 8,
-                       256);
+    int rc = shape_for(k_adjoint<D, BVH, ND, WL>, S, D, BVH, want_cdf, sh, adj_thread_bytes<D>(want_acc), 256);
     if (rc) return rc;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
