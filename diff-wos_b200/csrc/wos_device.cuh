@@ -602,12 +602,15 @@ __device__ __forceinline__ void wdescend(const SceneView &S, const float *q, int
     if (child < S.wt_count[L]) d = node_bound<D, L>(S, child, q);
     unsigned key = frontier_key(d, lane);
     wk.nb += 1;
+    unsigned mk = __reduce_min_sync(FULL, key);
     for (;;) {
-        const unsigned mk = __reduce_min_sync(FULL, key);
         if (key_dist(mk) > wt_bound(best.d2, tol2)) return;
         const int j = (int)(mk & 31u);
         if (lane == j) key = KEY_TAKEN;
         const int node = first + j;
+        // the next frontier entry, reduced before this node's work (whose
+        // pruning cannot change the frontier) so that its latency overlaps it
+        mk = __reduce_min_sync(FULL, key);
         if constexpr (L == 1) {
             wk.np += 1;
             const int s = node * WT_LEAF + lane;
@@ -671,12 +674,13 @@ __device__ __forceinline__ bool wball_descend(const SceneView &S, const float *q
     if (child < S.wt_count[L]) d = node_bound<D, L>(S, child, q);
     unsigned key = frontier_key(d, lane);
     wk.nb += 1;
+    unsigned mk = __reduce_min_sync(FULL, key);
     for (;;) {
-        const unsigned mk = __reduce_min_sync(FULL, key);
         if (key_dist(mk) > bound) return false;
         const int j = (int)(mk & 31u);
         if (lane == j) key = KEY_TAKEN;
         const int node = first + j;
+        mk = __reduce_min_sync(FULL, key);
         if constexpr (L == 1) {
             wk.np += 1;
             const int s = node * WT_LEAF + lane;
