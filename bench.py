@@ -260,7 +260,7 @@ def workload_config(npts, per_step_points=None):
 
 # ---------------------------------------------------------------- batched workload
 def batched_main(args):
-    """Many scenes in one persistent launch per dimension (graph replay):
+    """Many scenes in one plan: persistent launches per dimension and tree depth (graph replay):
     seeded random stars and noise-displaced icospheres, harmonic-polynomial
     boundary data, forward + adjoint of mean((u - exact)^2) per scene.
     Compared with the reference-shaped plain kernel run scene by scene."""
@@ -377,7 +377,7 @@ def batched_main(args):
         "config": {"workload": f"batched_{len(items)}_scenes_scale{args.scale:g}", "scenes": len(items),
                    "points": info["points"], "walks": info["walks"], "nsteps": 64, "epsilon": 1e-3,
                    "loss": "sum over scenes of mean((u - exact)^2); adjoint wrt vertices and values",
-                   "launch": "one persistent kernel per dimension and phase, CUDA graph replay",
+                   "launch": "one persistent kernel per dimension, tree depth and phase, CUDA graph replay",
                    "l2": "256 MiB buffer written between timed steps (L2 flush)"},
         "walks_per_s": info["walks"] / (ms * 1e-3),
         "autotuned_launch": {"block_threads": best[0], "chunk": best[1],

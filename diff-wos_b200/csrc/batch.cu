@@ -1,10 +1,13 @@
 // Batched multi-scene forward + adjoint: the wos_batch_* entry points.
 //
 // A plan holds many (scene, query set) items.  Items are grouped by
-// dimension; each group runs as one persistent work-queue launch per phase
-// (forward walks, per-point reduction, loss, adjoint) over the concatenation
-// of its items' walks, and the whole sequence is captured once into a CUDA
-// graph that later runs replay with a single launch.
+// dimension, and within a group ordered by tree depth; each group runs its
+// phases (forward walks, per-point reduction, loss, adjoint) over the
+// concatenation of its items' walks: the walk phases as one persistent
+// work-queue launch per run of items of equal depth (each compiled for that
+// depth), the reductions as one launch per group.  The whole sequence is
+// captured once into a CUDA graph that later runs replay with a single
+// launch.
 #include <algorithm>
 #include <string>
 #include <vector>
@@ -17,8 +20,16 @@ namespace wosd {
 
 static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// Consecutive items of a group whose trees have the same depth.
+struct BatchRun {
+    int wl = 0;  // specialised_depth of the items' trees
+    int first = 0, count = 0;
+    long long base = 0, walks = 0;
+};
+
 struct BatchGroup {
     int dim = 0;
+    std::vector<BatchRun> runs;
     std::vector<int> user_index;  // item index in the caller's list
     std::vector<BatchItemDev> items;
     std::vector<SceneView> views;
@@ -95,15 +106,18 @@ static int enqueue(wos_batch_s *b, cudaStream_t st) {
         if (b->want_adjoint) BT(cudaMemsetAsync(g.acc, 0, sizeof(double) * g.acc_len, st));
         WalkOut o{g.vals, nullptr, b->want_adjoint ? g.wrec : nullptr, b->want_adjoint ? g.wds : nullptr,
                   nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-        if (int rc = launch_walk_batch(g.dim, g.d_views, g.d_cfgs, g.d_items, n_items, g.walks, b->launch, o,
-                                       g.counters, st))
-            return rc;
+        for (const BatchRun &r : g.runs)
+            if (int rc = launch_walk_batch(g.dim, r.wl, g.d_views + r.first, g.d_cfgs + r.first, g.d_items + r.first,
+                                           r.count, r.base, r.walks, b->launch, o, g.counters, st))
+                return rc;
         if (int rc = launch_reduce_batch(g.vals, g.d_items, n_items, g.points, g.mean, g.var, st)) return rc;
         if (int rc = launch_loss_batch(g.mean, g.d_items, n_items, g.dLdu, g.loss, st)) return rc;
         if (b->want_adjoint) {
-            if (int rc = launch_adjoint_batch(g.dim, g.d_views, g.d_cfgs, a, g.d_items, n_items, g.walks, g.dLdu,
-                                              g.wrec, g.wds, g.acc, b->launch, g.counters + 1, st))
-                return rc;
+            for (const BatchRun &r : g.runs)
+                if (int rc = launch_adjoint_batch(g.dim, r.wl, g.d_views + r.first, g.d_cfgs + r.first, a,
+                                                  g.d_items + r.first, r.count, r.base, r.walks, g.dLdu, g.wrec,
+                                                  g.wds, g.acc, b->launch, g.counters + 1, st))
+                    return rc;
             if (int rc = launch_acc_to_f32(g.acc, g.grad, g.acc_len, st)) return rc;
         }
     }
@@ -147,12 +161,19 @@ int wos_batch_create(const wos_batch_item *items, int n_items, const wos_adjoint
     BatchGroup g2, g3;
     g2.dim = 2;
     g3.dim = 3;
-    for (int i = 0; i < n_items; ++i) {
-        const wos_batch_item &it = items[i];
-        if (it.scene == nullptr) {
+    for (int i = 0; i < n_items; ++i)
+        if (items[i].scene == nullptr) {
             delete b;
             return fail(WOS_ERR_INVALID_ARGUMENT, "item " + std::to_string(i) + ": scene is NULL");
         }
+    // within a dimension, items in order of tree depth (then caller order), so
+    // that each depth is one contiguous run of walks
+    std::vector<int> order(n_items);
+    for (int i = 0; i < n_items; ++i) order[i] = i;
+    auto depth = [&](int i) { return specialised_depth(items[i].scene->impl.wt_levels); };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return depth(x) < depth(y); });
+    for (int i : order) {
+        const wos_batch_item &it = items[i];
         const wos_params &p = it.params;
         if (p.nwalks < 1 || p.nsteps < 0 || !(p.epsilon >= 0.0f) || it.n < 0 || it.loss_kind < 0 ||
             it.loss_kind > 2 || (it.loss_kind != 1 && it.target_or_dLdu == nullptr && it.n > 0) ||
@@ -177,6 +198,16 @@ int wos_batch_create(const wos_batch_item *items, int n_items, const wos_adjoint
         g.acc_len += S.nV;
         d.ds_off = g.acc_len;
         g.acc_len += 5;
+        const int wl = specialised_depth(S.wt_levels);
+        if (g.runs.empty() || g.runs.back().wl != wl) {
+            BatchRun r;
+            r.wl = wl;
+            r.first = (int)g.items.size();
+            r.base = g.walks;
+            g.runs.push_back(r);
+        }
+        g.runs.back().count += 1;
+        g.runs.back().walks += (long long)it.n * p.nwalks;
         g.items.push_back(d);
         g.scenes.push_back(it.scene);
         g.views.push_back(S.view());

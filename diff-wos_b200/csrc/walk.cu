@@ -1196,9 +1196,6 @@ static int shape_for(Kern kern, const SceneImpl &S, int D, bool bvh, bool want_c
     return 0;
 }
 
-// Tree depths with their own kernel instance; deeper trees use the
-// any-depth instance (WL = 0).
-constexpr int WT_SPECIALISED_LEVELS = 3;
 
 template <int D, bool BVH, int WL>
 static int launch_walk_t(const SceneImpl &S, const float *P, long long total, const wos_params &p, bool records,
@@ -1231,7 +1228,7 @@ int launch_walk(const SceneImpl &S, const float *P, long long total, const wos_p
                 const WalkOut &out, unsigned long long *counter, cudaStream_t st) {
     if (total == 0) return 0;
     const bool bvh = p.use_bvh != 0;
-    const int wl = S.wt_levels <= WT_SPECIALISED_LEVELS ? S.wt_levels : 0;
+    const int wl = specialised_depth(S.wt_levels);
 #define WOS_WALK(D_)                                                                        \
     if (!bvh) return launch_walk_t<D_, false, 0>(S, P, total, p, records, out, counter, st); \
     switch (wl) {                                                                           \
@@ -1601,7 +1598,7 @@ int launch_adjoint(const SceneImpl &S, const float *P, long long total, const wo
                    const float *dLdu, int mode, const AdjOut &out, unsigned long long *counter, cudaStream_t st) {
     if (total == 0) return 0;
     const bool bvh = p.use_bvh != 0;
-    const int wl = S.wt_levels <= WT_SPECIALISED_LEVELS ? S.wt_levels : 0;
+    const int wl = specialised_depth(S.wt_levels);
 #define WOS_ADJ_M(D_, B_, W_)                                                                                   \
     switch (mode) {                                                                                             \
         case ADJ_ND_ONLY: return launch_adjoint_t<D_, B_, ADJ_ND_ONLY, W_>(S, P, total, p, a, dLdu, out, counter, st); \
@@ -1669,7 +1666,7 @@ __device__ __forceinline__ int find_item_point(const BatchItemDev *__restrict__ 
     return lo;
 }
 
-template <int D>
+template <int D, int WL = 0>
 __device__ __forceinline__ Hit warp_queries_batch(const SceneView *__restrict__ views, bool active, int item,
                                                   const float *x, int warm, Work &work, float ball_m = -1.0f) {
     const unsigned FULL = 0xffffffffu;
@@ -1689,25 +1686,27 @@ __device__ __forceinline__ Hit warp_queries_batch(const SceneView *__restrict__ 
         const SceneView &Sj = views[it];
         Hit h{-1, INFINITY};
         if (bm > 0.0f) {
-            wball<D>(Sj, q, bm, h, work);
+            wball<D, WL>(Sj, q, bm, h, work);
         } else {
             if (wp >= 0) {
                 h.prim = wp;
                 h.d2 = prim_d2<D>(Sj, wp, q);
             }
-            h = wquery<D>(Sj, q, h, work);
+            h = wquery<D, WL>(Sj, q, h, work);
         }
         if (lane == j) mine = h;
     }
     return mine;
 }
 
-template <int D>
+// One launch covers a run of items whose walks occupy [base, base + total)
+// of the group's walk index space; WL > 0: every item's tree has WL levels.
+template <int D, int WL>
 __global__ void __launch_bounds__(512) k_walk_batch(const SceneView *__restrict__ views,
                                                    const WalkCfg *__restrict__ cfgs,
                                                    const BatchItemDev *__restrict__ items, int n_items,
-                                                   long long total, unsigned long long *counter, int chunk,
-                                                   WalkOut out, int count_work) {
+                                                   long long base, long long total, unsigned long long *counter,
+                                                   int chunk, WalkOut out, int count_work) {
     Queue q{0, 0, false};
     bool active = false;
     long long idx = 0;
@@ -1720,6 +1719,7 @@ __global__ void __launch_bounds__(512) k_walk_batch(const SceneView *__restrict_
         const bool was = active;
         if (!refill(q, active, idx, counter, total, chunk)) break;
         if (active && !was) {
+            idx += base;
             item = find_item(items, n_items, idx);
             const BatchItemDev &it = items[item];
             const long long local = idx - it.walk_begin;
@@ -1729,7 +1729,7 @@ __global__ void __launch_bounds__(512) k_walk_batch(const SceneView *__restrict_
             walk_origin<D>(cfgs[item], it.P, pt, wk, x0);
             w.start(x0, D);
         }
-        const Hit hit = warp_queries_batch<D>(views, active, item, w.p, w.last, work);
+        const Hit hit = warp_queries_batch<D, WL>(views, active, item, w.p, w.last, work);
         if (!active) continue;
         const SceneView &S = views[item];
         const WalkCfg &c = cfgs[item];
@@ -1821,10 +1821,11 @@ __global__ void k_loss_batch(const double *__restrict__ mean, const BatchItemDev
 
 // Adjoint of every item, starting from the forward records.  Gradients go to
 // per-item FP64 accumulators (acc + it.dV_off / dg_off / ds_off).
-template <int D>
+template <int D, int WL>
 __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
     const SceneView *__restrict__ views, const WalkCfg *__restrict__ cfgs, AdjCfg a,
-    const BatchItemDev *__restrict__ items, int n_items, long long total, const float *__restrict__ dLdu,
+    const BatchItemDev *__restrict__ items, int n_items, long long base, long long total,
+    const float *__restrict__ dLdu,
     unsigned long long *counter, int chunk, const int *__restrict__ wrec, const float *__restrict__ wds, double *acc,
     int count_work) {
     extern __shared__ float4 smem[];
@@ -1857,6 +1858,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
         const bool was = active;
         if (!refill(q, active, idx, counter, total, chunk)) break;
         if (active && !was) {
+            idx += base;
             item = find_item(items, n_items, idx);
             const BatchItemDev &it = items[item];
             const SceneView &S = views[item];
@@ -1932,7 +1934,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
         Hit pre{-1, INFINITY};
         if (active && phase == PH_BALL)
             ball_precheck<D>(views[item], qpos, (ba + bb) * 0.5f, bwarm, rprim, need, ball_m, pre);
-        Hit hit = warp_queries_batch<D>(views, need, item, x, walking ? w.last : rprim, work, ball_m);
+        Hit hit = warp_queries_batch<D, WL>(views, need, item, x, walking ? w.last : rprim, work, ball_m);
         if (!active) continue;
         if (phase == PH_BALL && (!need || (ball_m > 0.0f && hit.prim < 0))) hit = pre;
         const SceneView &S = views[item];
@@ -2047,47 +2049,71 @@ static int persistent_grid(Kern kern, int block, size_t smem, int blocks_per_sm,
     return 0;
 }
 
-int launch_walk_batch(int D, const SceneView *views, const WalkCfg *cfgs, const BatchItemDev *items, int n_items,
-                      long long total, const BatchLaunch &L, const WalkOut &out, unsigned long long *counter,
-                      cudaStream_t st) {
+template <int D, int WL>
+static int launch_walk_batch_t(const SceneView *views, const WalkCfg *cfgs, const BatchItemDev *items, int n_items,
+                               long long base, long long total, const BatchLaunch &L, const WalkOut &out,
+                               unsigned long long *counter, cudaStream_t st) {
+    int grid = 0;
+    if (int rc = persistent_grid(k_walk_batch<D, WL>, L.block, 0, L.blocks_per_sm, grid)) return rc;
+    k_walk_batch<D, WL><<<grid, L.block, 0, st>>>(views, cfgs, items, n_items, base, total, counter, L.chunk, out,
+                                                  L.count_work);
+    return 0;
+}
+
+int launch_walk_batch(int D, int wl, const SceneView *views, const WalkCfg *cfgs, const BatchItemDev *items,
+                      int n_items, long long base, long long total, const BatchLaunch &L, const WalkOut &out,
+                      unsigned long long *counter, cudaStream_t st) {
     if (total == 0 || n_items == 0) return 0;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
-    int grid = 0;
+    static_assert(WT_SPECIALISED_LEVELS == 3, "one instance per specialised depth");
+    int rc = 0;
+#define WOS_WB(DD, WW) rc = launch_walk_batch_t<DD, WW>(views, cfgs, items, n_items, base, total, L, out, counter, st)
     if (D == 2) {
-        if (int rc = persistent_grid(k_walk_batch<2>, L.block, 0, L.blocks_per_sm, grid)) return rc;
-        k_walk_batch<2><<<grid, L.block, 0, st>>>(views, cfgs, items, n_items, total, counter, L.chunk, out,
-                                                  L.count_work);
+        if (wl == 1) WOS_WB(2, 1); else if (wl == 2) WOS_WB(2, 2); else if (wl == 3) WOS_WB(2, 3); else WOS_WB(2, 0);
     } else {
-        if (int rc = persistent_grid(k_walk_batch<3>, L.block, 0, L.blocks_per_sm, grid)) return rc;
-        k_walk_batch<3><<<grid, L.block, 0, st>>>(views, cfgs, items, n_items, total, counter, L.chunk, out,
-                                                  L.count_work);
+        if (wl == 1) WOS_WB(3, 1); else if (wl == 2) WOS_WB(3, 2); else if (wl == 3) WOS_WB(3, 3); else WOS_WB(3, 0);
     }
+#undef WOS_WB
+    if (rc) return rc;
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail_cuda(e, "k_walk_batch launch");
     return 0;
 }
 
-int launch_adjoint_batch(int D, const SceneView *views, const WalkCfg *cfgs, const AdjCfg &a,
-                         const BatchItemDev *items, int n_items, long long total, const float *dLdu,
-                         const int *wrec, const float *wds, double *acc, const BatchLaunch &L,
+template <int D, int WL>
+static int launch_adjoint_batch_t(const SceneView *views, const WalkCfg *cfgs, const AdjCfg &a,
+                                  const BatchItemDev *items, int n_items, long long base, long long total,
+                                  const float *dLdu, const int *wrec, const float *wds, double *acc,
+                                  const BatchLaunch &L, unsigned long long *counter, cudaStream_t st) {
+    const int block = std::min(L.block, 256);
+    const size_t smem = (size_t)block * adj_thread_bytes<D>(true) + 16;
+    const int chunk = std::max(1, L.chunk / 2);
+    int grid = 0;
+    if (int rc = persistent_grid(k_adjoint_batch<D, WL>, block, smem, L.blocks_per_sm, grid)) return rc;
+    k_adjoint_batch<D, WL><<<grid, block, smem, st>>>(views, cfgs, a, items, n_items, base, total, dLdu, counter,
+                                                      chunk, wrec, wds, acc, L.count_work);
+    return 0;
+}
+
+int launch_adjoint_batch(int D, int wl, const SceneView *views, const WalkCfg *cfgs, const AdjCfg &a,
+                         const BatchItemDev *items, int n_items, long long base, long long total,
+                         const float *dLdu, const int *wrec, const float *wds, double *acc, const BatchLaunch &L,
                          unsigned long long *counter, cudaStream_t st) {
     if (total == 0 || n_items == 0) return 0;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
-    const int block = std::min(L.block, 256);
-    const size_t smem = (size_t)block * (D == 2 ? adj_thread_bytes<2>(true) : adj_thread_bytes<3>(true)) + 16;
-    const int chunk = std::max(1, L.chunk / 2);
-    int grid = 0;
+    int rc = 0;
+#define WOS_AB(DD, WW)                                                                                        \
+    rc = launch_adjoint_batch_t<DD, WW>(views, cfgs, a, items, n_items, base, total, dLdu, wrec, wds, acc, L, \
+                                        counter, st)
     if (D == 2) {
-        if (int rc = persistent_grid(k_adjoint_batch<2>, block, smem, L.blocks_per_sm, grid)) return rc;
-        k_adjoint_batch<2><<<grid, block, smem, st>>>(views, cfgs, a, items, n_items, total, dLdu, counter, chunk,
-                                                      wrec, wds, acc, L.count_work);
+        if (wl == 1) WOS_AB(2, 1); else if (wl == 2) WOS_AB(2, 2); else if (wl == 3) WOS_AB(2, 3); else WOS_AB(2, 0);
     } else {
-        if (int rc = persistent_grid(k_adjoint_batch<3>, block, smem, L.blocks_per_sm, grid)) return rc;
-        k_adjoint_batch<3><<<grid, block, smem, st>>>(views, cfgs, a, items, n_items, total, dLdu, counter, chunk,
-                                                      wrec, wds, acc, L.count_work);
+        if (wl == 1) WOS_AB(3, 1); else if (wl == 2) WOS_AB(3, 2); else if (wl == 3) WOS_AB(3, 3); else WOS_AB(3, 0);
     }
+#undef WOS_AB
+    if (rc) return rc;
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail_cuda(e, "k_adjoint_batch launch");
     return 0;

@@ -83,12 +83,21 @@ struct BatchLaunch {
 
 WalkCfg make_cfg(const wos_params &p);
 AdjCfg make_adj_cfg(const wos_adjoint_params &a);
-int launch_walk_batch(int D, const SceneView *views, const WalkCfg *cfgs, const BatchItemDev *items, int n_items,
-                      long long total, const BatchLaunch &L, const WalkOut &out, unsigned long long *counter,
-                      cudaStream_t st);
-int launch_adjoint_batch(int D, const SceneView *views, const WalkCfg *cfgs, const AdjCfg &a,
-                         const BatchItemDev *items, int n_items, long long total, const float *dLdu,
-                         const int *wrec, const float *wds, double *acc, const BatchLaunch &L,
+// Tree depths with their own kernel instance; deeper trees use the
+// any-depth instance (depth argument 0).
+constexpr int WT_SPECIALISED_LEVELS = 3;
+inline int specialised_depth(int wt_levels) { return wt_levels <= WT_SPECIALISED_LEVELS ? wt_levels : 0; }
+
+// A batch launch covers items [0, n_items) of `items` / `views` / `cfgs`
+// (callers pass pointers offset to a run of items) whose walks are
+// [base, base + total) of the group's walk index space; wl: the run's
+// common tree depth (specialised_depth), 0 for mixed or deep trees.
+int launch_walk_batch(int D, int wl, const SceneView *views, const WalkCfg *cfgs, const BatchItemDev *items,
+                      int n_items, long long base, long long total, const BatchLaunch &L, const WalkOut &out,
+                      unsigned long long *counter, cudaStream_t st);
+int launch_adjoint_batch(int D, int wl, const SceneView *views, const WalkCfg *cfgs, const AdjCfg &a,
+                         const BatchItemDev *items, int n_items, long long base, long long total,
+                         const float *dLdu, const int *wrec, const float *wds, double *acc, const BatchLaunch &L,
                          unsigned long long *counter, cudaStream_t st);
 int launch_reduce_batch(const float *vals, const BatchItemDev *items, int n_items, int n_points, double *mean,
                         double *var, cudaStream_t st);
