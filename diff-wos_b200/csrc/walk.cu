@@ -1829,12 +1829,17 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
     unsigned long long *counter, int chunk, const int *__restrict__ wrec, const float *__restrict__ wds, double *acc,
     int count_work) {
     extern __shared__ float4 smem[];
-    const AdjSmem<D> am = adj_smem<D>(reinterpret_cast<double *>(smem), true);
+    // source-gradient accumulators only when the launch has source derivatives
+    // (the launcher sizes shared memory the same way)
+    const bool acc_on = wds != nullptr;
+    const AdjSmem<D> am = adj_smem<D>(reinterpret_cast<double *>(smem), acc_on);
     AdjSlot<D> &slot = *am.slot;
     double *acc_src = am.acc;  // k-th accumulator at acc_src[k * blockDim.x]
     const int AS = blockDim.x;
+    if (acc_on) {
 #pragma unroll
-    for (int k = 0; k < 5; ++k) acc_src[k * AS] = 0.0;
+        for (int k = 0; k < 5; ++k) acc_src[k * AS] = 0.0;
+    }
     int acc_item = -1;  // item whose source gradient acc_src holds
     NdState<D> &st = slot.st;
     float *rn = st.rn;
@@ -2087,7 +2092,7 @@ static int launch_adjoint_batch_t(const SceneView *views, const WalkCfg *cfgs, c
                                   const float *dLdu, const int *wrec, const float *wds, double *acc,
                                   const BatchLaunch &L, unsigned long long *counter, cudaStream_t st) {
     const int block = std::min(L.block, 256);
-    const size_t smem = (size_t)block * adj_thread_bytes<D>(true) + 16;
+    const size_t smem = (size_t)block * adj_thread_bytes<D>(wds != nullptr) + 16;
     const int chunk = std::max(1, L.chunk / 2);
     int grid = 0;
     if (int rc = persistent_grid(k_adjoint_batch<D, WL>, block, smem, L.blocks_per_sm, grid)) return rc;
