@@ -1102,7 +1102,7 @@ __global__ void k_add_f64_to_f32(const double *src, float *dst, long long n) {
 }
 
 // ------------------------------------------------------------------ host
-static wos_launch_config g_cfg[2] = {{256, 0, 64, 1024}, {256, 0, 32, 768}};
+static wos_launch_config g_cfg[2] = {{256, 0, 64, 1024}, {256, 0, 16, 768}};
 
 int set_launch_config(int dim, const wos_launch_config *cfg) {
     if (dim != 2 && dim != 3) return fail(WOS_ERR_INVALID_ARGUMENT, "dim must be 2 or 3");
