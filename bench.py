@@ -484,6 +484,7 @@ def c3_main(args):
         "accuracy": {"rmse_vs_exact": float(np.sqrt((err ** 2).mean())), "rms_standard_error":
                      float(np.sqrt((se ** 2).mean())),
                      "truncated_fraction": float((steps.cpu().numpy() >= 64).mean())},
+        "walk_steps": walk_steps(steps, 64),
         "device_status": wos.device_status(),
     }
     if clk is not None:
@@ -730,6 +731,9 @@ def main():
 
     # -- plain (reference-shaped) forward kernel vs the persistent one, same walks
     plain = plain_vs_persistent(scene, P_d, n)
+    # -- steps per walk on a sample of points (untimed)
+    _, st = scene.values(P_d[: max(1, (1 << 18) // NWALKS)], walk_settings(3), want_steps=True)
+    steps_stats = walk_steps(st, NSTEPS)
 
     hbm, peak_kind = peaks()
     adj_avg = float(np.mean(t_adj))
@@ -752,6 +756,7 @@ def main():
         "gpu_launches": args.steps * 7,
         "device_status": status,
         "plain_vs_persistent": plain,
+        "walk_steps": steps_stats,
         "tree_work_per_launch": {"adjoint": adj_work, "forward": fwd_work,
                                  "note": "this build's wide-tree counters: queries, node expansions and leaf "
                                          "steps (one warp step each)"},
@@ -789,6 +794,21 @@ def main():
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def walk_steps(steps, nsteps):
+    """Steps-per-walk statistics of a sample of walks: quantiles, a histogram
+    over power-of-two bins, and the fraction truncated at nsteps."""
+    s = steps.reshape(-1).cpu().numpy()
+    edges = [0, 4, 8, 16, 32, nsteps - 1]
+    hist, lo = {}, 0
+    for e in edges[1:]:
+        hist[f"{lo + (1 if lo else 0)}-{e}"] = float(((s > lo) & (s <= e)).mean()) if lo else float((s <= e).mean())
+        lo = e
+    hist[f">={nsteps}"] = float((s >= nsteps).mean())
+    return {"walks": int(s.size), "mean": float(s.mean()), "p50": float(np.percentile(s, 50)),
+            "p90": float(np.percentile(s, 90)), "p99": float(np.percentile(s, 99)), "histogram": hist,
+            "truncated_fraction": float((s >= nsteps).mean())}
 
 
 def plain_vs_persistent(scene, P_d, n):
