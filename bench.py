@@ -731,8 +731,9 @@ def main():
 
     # -- plain (reference-shaped) forward kernel vs the persistent one, same walks
     plain = plain_vs_persistent(scene, P_d, n)
-    # -- steps per walk on a sample of points (untimed)
-    _, st = scene.values(P_d[: max(1, (1 << 18) // NWALKS)], walk_settings(3), want_steps=True)
+    # -- steps per walk on a sample of points spread over the grid (untimed)
+    stride = max(1, n // max(1, (1 << 18) // NWALKS))
+    _, st = scene.values(P_d[::stride].contiguous(), walk_settings(3), want_steps=True)
     steps_stats = walk_steps(st, NSTEPS)
 
     hbm, peak_kind = peaks()
