@@ -357,8 +357,11 @@ typedef struct wos_batch_item {
 typedef struct wos_batch_s *wos_batch_t;
 
 /* Plan a batched forward (+ adjoint if want_adjoint) over many items: items
- * of one dimension run as one persistent work-queue launch per phase over the
- * concatenation of their walks, in item order (order the items scene-major).
+ * of one dimension form a group whose walks are concatenated in order of the
+ * scenes' tree depth, then item order (order the items scene-major); each
+ * walk phase runs one persistent work-queue launch per run of equal depth
+ * (compiled for that depth), the reductions one launch per group.
+ * wos_batch_info reports the number of groups (dimensions present).
  * Buffers for all outputs are owned by the plan (wos_batch_outputs).  This
  * is the batched form of wos_solve_adjoint; no counterpart in the reference,
  * whose callers loop over scenes with one thrust launch each
