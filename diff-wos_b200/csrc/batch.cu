@@ -284,6 +284,59 @@ int wos_batch_set_launch(wos_batch_t b, int block_threads, int blocks_per_sm, in
     return 0;
 }
 
+int wos_batch_autotune(wos_batch_t b, const int32_t *block_threads, const int32_t *chunk, int n_candidates,
+                       int repeats, wos_stream_t stream, float *ms, int32_t *best) {
+    if (b == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "batch is NULL");
+    if (block_threads == nullptr || chunk == nullptr || n_candidates < 1 || repeats < 1)
+        return fail(WOS_ERR_INVALID_ARGUMENT, "autotune needs candidates and repeats >= 1");
+    for (int i = 0; i < n_candidates; ++i)
+        if (block_threads[i] % 32 || block_threads[i] < 32 || block_threads[i] > 512 || chunk[i] < 1)
+            return fail(WOS_ERR_INVALID_ARGUMENT, "candidate " + std::to_string(i) + ": invalid launch shape");
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    BT(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return fail(WOS_ERR_INVALID_ARGUMENT, "autotune during stream capture");
+    const BatchLaunch keep = b->launch;
+    b->launch.count_work = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    BT(cudaEventCreate(&e0));
+    cudaError_t e = cudaEventCreate(&e1);
+    if (e != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail_cuda(e, "cudaEventCreate");
+    }
+    int rc = 0, arg = -1;
+    float best_ms = INFINITY;
+    for (int i = 0; i < n_candidates && !rc; ++i) {
+        b->launch.block = block_threads[i];
+        b->launch.chunk = chunk[i];
+        float t = INFINITY;
+        for (int r = 0; r <= repeats && !rc; ++r) {
+            if ((e = cudaEventRecord(e0, st)) != cudaSuccess) rc = fail_cuda(e, "cudaEventRecord");
+            if (!rc) rc = enqueue(b, st);
+            if (!rc && (e = cudaEventRecord(e1, st)) != cudaSuccess) rc = fail_cuda(e, "cudaEventRecord");
+            if (!rc && (e = cudaEventSynchronize(e1)) != cudaSuccess) rc = fail_cuda(e, "cudaEventSynchronize");
+            float x = 0.0f;
+            if (!rc && (e = cudaEventElapsedTime(&x, e0, e1)) != cudaSuccess) rc = fail_cuda(e, "cudaEventElapsedTime");
+            if (!rc && r > 0) t = std::min(t, x);  // r = 0 is the untimed step
+        }
+        if (ms) ms[i] = t;
+        if (!rc && t < best_ms) {
+            best_ms = t;
+            arg = i;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->launch = keep;
+    if (rc) return rc;
+    b->launch.block = block_threads[arg];
+    b->launch.chunk = chunk[arg];
+    drop_graph(b);
+    if (best) *best = arg;
+    return 0;
+}
+
 int wos_batch_refresh(wos_batch_t b, wos_stream_t stream) {
     if (b == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "batch is NULL");
     drop_graph(b);

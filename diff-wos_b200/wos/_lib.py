@@ -169,6 +169,7 @@ SIGNATURES = {
     "wos_batch_create": (_I, [ctypes.POINTER(WosBatchItem), _I, ctypes.POINTER(WosAdjointParams), _I, _P,
                               ctypes.POINTER(_P)]),
     "wos_batch_set_launch": (_I, [_P, _I, _I, _I]),
+    "wos_batch_autotune": (_I, [_P, _P, _P, _I, _I, _P, _P, _P]),
     "wos_batch_refresh": (_I, [_P, _P]),
     "wos_batch_run": (_I, [_P, _I, _P]),
     "wos_batch_outputs": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),

@@ -84,11 +84,6 @@ def tune_scene(native, P, settings, adjoint=None, candidates=None, repeats: int 
 
 
 def tune_batch(plan, candidates=None, repeats: int = 1):
-    """Pick the launch shape of a BatchPlan by timing whole steps."""
-    times = {}
-    for bt, chunk in candidates or CANDIDATES:
-        plan.set_launch(bt, 0, chunk)
-        times[(bt, chunk)] = _time(lambda: plan.run(use_graph=False), repeats)
-    best = min(times, key=times.get)
-    plan.set_launch(best[0], 0, best[1])
-    return best, times
+    """Pick the launch shape of a BatchPlan by timing whole steps (the
+    library's wos_batch_autotune, on the current stream)."""
+    return plan.autotune(candidates or CANDIDATES, repeats)

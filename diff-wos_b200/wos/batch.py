@@ -51,6 +51,18 @@ class BatchPlan:
     def set_launch(self, block_threads=256, blocks_per_sm=0, chunk=64):
         call("wos_batch_set_launch", self.h, int(block_threads), int(blocks_per_sm), int(chunk))
 
+    def autotune(self, candidates, repeats: int = 1):
+        """Time whole steps for each (block_threads, chunk) candidate and keep
+        the fastest (wos_batch_autotune).  Returns (best, {candidate: ms})."""
+        n = len(candidates)
+        bt = (ctypes.c_int32 * n)(*[int(c[0]) for c in candidates])
+        ch = (ctypes.c_int32 * n)(*[int(c[1]) for c in candidates])
+        ms = (ctypes.c_float * n)()
+        best = ctypes.c_int32()
+        call("wos_batch_autotune", self.h, bt, ch, n, int(repeats), stream(), ms, ctypes.byref(best))
+        cands = [tuple(int(x) for x in c) for c in candidates]
+        return cands[best.value], {c: float(ms[i]) for i, c in enumerate(cands)}
+
     def refresh(self):
         call("wos_batch_refresh", self.h, stream())
 

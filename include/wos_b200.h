@@ -372,6 +372,17 @@ WOS_API int wos_batch_create(const wos_batch_item *items, int n_items, const wos
 /* Launch shape of the batch kernels (see wos_launch_config). */
 WOS_API int wos_batch_set_launch(wos_batch_t b, int block_threads, int blocks_per_sm, int chunk);
 
+/* Launch-shape autotuner: times whole steps of the plan (no graph) for each
+ * candidate (block_threads[i], chunk[i]) on `stream` with CUDA events -- one
+ * untimed step, then the best of `repeats` -- and keeps the fastest with
+ * wos_batch_set_launch (blocks per SM unchanged).  Results do not depend on
+ * the shape, only speed does.  ms (n_candidates floats, may be NULL) gets each
+ * candidate's time, *best its index.  Synchronises the stream, so it must not
+ * be called while the stream is being captured.  This library's own tuner;
+ * no counterpart in the reference, whose launch shape is fixed. */
+WOS_API int wos_batch_autotune(wos_batch_t b, const int32_t *block_threads, const int32_t *chunk, int n_candidates,
+                               int repeats, wos_stream_t stream, float *ms, int32_t *best);
+
 /* Re-read the scenes' device views (after wos_scene_update_vertices). */
 WOS_API int wos_batch_refresh(wos_batch_t b, wos_stream_t stream);
 
