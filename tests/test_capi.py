@@ -67,6 +67,12 @@ def test_argument_validation_without_gpu():
         _lib.WOS_ERR_INVALID_ARGUMENT
     assert b"nwalks" in L.wos_last_error_string()
     assert L.wos_solve_workspace_size(10, ctypes.byref(_lib.WosParams(4, 32, 1e-3))) >= 10 * 4 * 4
+    bt = (ctypes.c_int32 * 1)(100)
+    ch = (ctypes.c_int32 * 1)(16)
+    assert L.wos_batch_autotune(None, bt, ch, 1, 1, None, None, None) == _lib.WOS_ERR_INVALID_ARGUMENT
+    assert L.wos_batch_autotune(ctypes.c_void_p(1), bt, ch, 0, 1, None, None, None) == _lib.WOS_ERR_INVALID_ARGUMENT
+    assert L.wos_batch_autotune(ctypes.c_void_p(1), bt, ch, 1, 1, None, None, None) == _lib.WOS_ERR_INVALID_ARGUMENT
+    assert b"candidate 0" in L.wos_last_error_string()
     assert L.wos_version() >= 100
 
 
