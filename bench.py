@@ -517,6 +517,105 @@ def inverse_run(scene, P, target, iters, nwalks, lr, dev, g0=None):
     return g.detach(), torch.cat(losses)
 
 
+def c1_main(args):
+    """The plain 2D primal solve: unit circle as a CCW polyline of 1024 equal
+    segments, g = x^3 - 3 x y^2 (harmonic, so u = g inside), no source; the
+    128^2 grid on [-0.9, 0.9]^2 masked to the interior (14,592 points), 64
+    walks per point, epsilon 1e-3, seed 0, nsteps 32 (and 256, reported
+    beside).  A step is the solve (walks + per-point FP64 mean / variance).
+    Beside it: RMSE against the closed form, the reference-shaped plain kernel
+    with LBVH and brute-force search, and the oracle on the host cores in both
+    search modes on a bounded sample."""
+    import torch
+    import wos
+    from wos import shapes
+    from wos.native import NativeScene, WalkSettings
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    V, F = shapes.circle(1024, 1.0)
+    g = shapes.harmonic_c1(V).astype(np.float32)
+    P = shapes.grid(128, -0.9, 0.9)
+    P = np.ascontiguousarray(P[(P.astype(np.float64) ** 2).sum(1) < 1.0]).astype(np.float32)
+    scene = NativeScene(V, F, g)
+    Pd = torch.as_tensor(P, device=dev)
+    n, nw = len(P), args.walks if args.walks is not None else 64
+    exact = shapes.harmonic_c1(P)
+
+    def ws(nsteps, seed, bvh=True):
+        return WalkSettings(nwalks=nw, nsteps=nsteps, epsilon=1e-3, seed=seed, use_bvh=bvh)
+
+    def timed(fn, reps):
+        for w in range(max(3, args.warmup)):
+            fn(w)
+        torch.cuda.synchronize()
+        t = 0.0
+        for k in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn(1000 + k)
+            b.record()
+            torch.cuda.synchronize()
+            t += a.elapsed_time(b) * 1e-3
+        return t
+
+    clocks = ClockSampler(None)
+    clocks.start()
+    t32 = timed(lambda k: scene.solve(Pd, ws(32, k)), args.steps)
+    clk = clocks.stop()
+    t256 = timed(lambda k: scene.solve(Pd, ws(256, k)), args.steps)
+    accuracy = {}
+    for ns in (32, 256):
+        mean, var = scene.solve(Pd, ws(ns, 0), want_var=True)
+        err = mean.cpu().numpy() - exact
+        accuracy[f"nsteps{ns}"] = {"rmse_vs_exact": float(np.sqrt((err ** 2).mean())),
+                                   "rms_standard_error": float(np.sqrt((var.cpu().numpy() / nw).mean()))}
+    _, st = scene.values(Pd, ws(32, 0), want_steps=True)
+    plain = {}
+    for name, bvh in (("lbvh", True), ("brute", False)):
+        tp = timed(lambda k: scene.values(Pd, ws(32, k, bvh), plain=True), 1)
+        plain[name + "_walks_per_s"] = n * nw / tp
+    # the oracle on the host cores, both search modes, bounded samples
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as O
+    S = O.OracleScene(V, F, g)
+    threads = os.cpu_count() or 1
+    cpu = {}
+    for name, bvh in (("bvh", True), ("brute", False)):
+        prm = O.make_params(nwalks=nw, nsteps=32, epsilon=1e-3, use_bvh=bvh, seed=0)
+        m = 64
+        while True:
+            sub = P[np.linspace(0, n - 1, m).astype(np.int64)]
+            t0 = time.perf_counter()
+            S.walk_values(sub, prm, nthreads=threads)
+            tc = time.perf_counter() - t0
+            if tc > 2.0 or m >= n:
+                break
+            m = min(n, m * 4)
+        cpu[name] = {"value": m * nw / tc, "unit": "walks/s", "cores": threads, "kind": "port",
+                     "sample": f"{m} of {n} points x {nw} walks, nsteps 32, {threads} threads, {cpu_info()}"}
+    walks = n * nw
+    line = {
+        "metric": "wos_walks_per_s", "value": walks * args.steps / t32, "unit": "walks/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": t32 / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"2d_primal_circle1024_grid128_walks{nw}", "points": n, "walks_per_point": nw,
+                   "nsteps": 32, "epsilon": 1e-3, "nearest": "LBVH",
+                   "l2": "inputs and scene (< 1 MB) stay in L2; every step reruns the same solve"},
+        "nsteps256_walks_per_s": walks * args.steps / t256,
+        "plain_kernel": plain,
+        "accuracy": accuracy,
+        "walk_steps": walk_steps(st, 32),
+        "cpu_baseline": cpu["bvh"],
+        "cpu_baseline_brute": cpu["brute"],
+        "device_status": wos.device_status(),
+    }
+    if clk is not None:
+        line["clocks"] = clk
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def c4_main(args):
     """The 2D inverse problem: star r = 0.6 + 0.25 cos 5 theta with 8192
     segments, unknown per-vertex g (initialised to 0), target = the solve with
@@ -587,9 +686,10 @@ def main():
     ap.add_argument("--grid", type=int, default=GRID, help="query grid (smaller only for profiling captures)")
     ap.add_argument("--walks", type=int, default=None,
                     help="walks per point (c2: 256, c3: 128; smaller only for profiling)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "batched"],
-                    help="c2: the 2D differentiable solve (default); c3: the 3D forward + adjoint solve; "
-                         "c4: the 2D inverse problem; batched: many scenes in one launch")
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "batched"],
+                    help="c2: the 2D differentiable solve (default); c1: the plain 2D primal solve; "
+                         "c3: the 3D forward + adjoint solve; c4: the 2D inverse problem; "
+                         "batched: many scenes in one launch")
     ap.add_argument("--iters", type=int, default=500, help="Adam iterations of the c4 workload")
     ap.add_argument("--points", type=int, default=1_000_000, help="query points of the c3 workload")
     ap.add_argument("--scale", type=float, default=0.1, help="query-count scale of the batched workload")
@@ -597,6 +697,8 @@ def main():
     set_size(args.grid, args.walks if args.walks is not None else NWALKS)
     if args.workload == "batched" and args.impl == "ours":
         return batched_main(args)
+    if args.workload == "c1" and args.impl == "ours":
+        return c1_main(args)
     if args.workload == "c3" and args.impl == "ours":
         return c3_main(args)
     if args.workload == "c4" and args.impl == "ours":
@@ -801,7 +903,7 @@ def walk_steps(steps, nsteps):
     """Steps-per-walk statistics of a sample of walks: quantiles, a histogram
     over power-of-two bins, and the fraction truncated at nsteps."""
     s = steps.reshape(-1).cpu().numpy()
-    edges = [0, 4, 8, 16, 32, nsteps - 1]
+    edges = [0] + [e for e in (4, 8, 16, 32) if e < nsteps - 1] + [nsteps - 1]
     hist, lo = {}, 0
     for e in edges[1:]:
         hist[f"{lo + (1 if lo else 0)}-{e}"] = float(((s > lo) & (s <= e)).mean()) if lo else float((s <= e).mean())
