@@ -397,6 +397,37 @@ def batched_main(args):
 
 
 # ---------------------------------------------------------------- 3D workload
+def c3_cpu_baseline(V, F, P, npts, nw, target_s=3.0):
+    """The oracle on the host cores (all threads) on bounded samples of the
+    same 3D step: forward + adjoint with its binary LBVH (walks/s, the GPU
+    line's unit), and the forward walk with the brute-force search (the
+    reference's default)."""
+    from wos import shapes
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as O
+    S = O.OracleScene(V, F, shapes.harmonic_c3(V).astype(np.float32))
+    threads = os.cpu_count() or 1
+    adj = O.make_adj(1e-3, 0.1, True, False, 1e-3, True, True, False)
+    out = {}
+    for name, bvh, with_adj, m in (("cpu_baseline", True, True, 4), ("cpu_baseline_brute_forward", False, False, 1)):
+        prm = O.make_params(nwalks=nw, nsteps=64, epsilon=1e-3, use_bvh=bvh, seed=0)
+        while True:
+            sub = P[:m]
+            t0 = time.perf_counter()
+            vals, _, _ = S.walk_values(sub, prm, nthreads=threads)
+            if with_adj:
+                mean, _ = O.reduce(vals)
+                S.adjoint(sub, prm, adj, (2.0 * mean / npts).astype(np.float32), nthreads=threads)
+            tc = time.perf_counter() - t0
+            if tc > target_s / 4 or m >= 4096:
+                break
+            m *= 4
+        what = "forward + adjoint" if with_adj else "forward only, brute-force search"
+        out[name] = {"value": m * nw / tc, "unit": "walks/s", "cores": threads, "kind": "port",
+                     "sample": f"{m} of {npts} points x {nw} walks ({what}), {threads} threads, {cpu_info()}"}
+    return out
+
+
 def c3_main(args):
     """The 3D forward + adjoint solve: icosphere subdivided to 81,920
     triangles, radially displaced by 0.15 x seeded 3-octave value noise,
@@ -489,6 +520,8 @@ def c3_main(args):
     }
     if clk is not None:
         line["clocks"] = clk
+    if not args.no_cpu_baseline:
+        line.update(c3_cpu_baseline(V, F, P.cpu().numpy(), npts, nw))
     print(json.dumps(line), flush=True)
     return 0
 
