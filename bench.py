@@ -391,9 +391,41 @@ def batched_main(args):
     }
     if clk is not None:
         line["clocks"] = clk
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = batched_cpu_baseline(scenes, items, exact)
     print(json.dumps(line), flush=True)
     plan.close()
     return 0
+
+
+def batched_cpu_baseline(scenes, items, exact, every=8, m=4):
+    """The oracle on the host cores (all threads, LBVH) for the batched step:
+    forward + adjoint of mean((u - exact)^2) on `m` points of every `every`-th
+    scene, each scene with its own walk count; the per-point time of each
+    sampled scene, weighted by that scene's point count, gives the workload's
+    query points/s."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    adj = O.make_adj(1e-3, 0.1, True, False, 1e-3, True, True, False)
+    pts, secs, walks = 0.0, 0.0, 0
+    for i in range(0, len(scenes), every):
+        sc, it = scenes[i], items[i]
+        S = O.OracleScene(sc["V"], sc["F"], sc["g"])
+        P = it.points[:m].cpu().numpy()
+        n = int(it.points.shape[0])
+        prm = O.make_params(nwalks=sc["nwalks"], nsteps=64, epsilon=1e-3, use_bvh=True, seed=sc["seed"])
+        t0 = time.perf_counter()
+        vals, _, _ = S.walk_values(P, prm, nthreads=threads)
+        mean, _ = O.reduce(vals)
+        S.adjoint(P, prm, adj, (2.0 * (mean - exact[i][:m]) / n).astype(np.float32), nthreads=threads)
+        t = time.perf_counter() - t0
+        pts += n
+        secs += n * t / len(P)
+        walks += len(P) * sc["nwalks"]
+    return {"value": pts / secs, "unit": "points/s", "cores": threads, "kind": "port",
+            "sample": f"{m} points of every {every}th scene ({walks} walks, forward + adjoint), times weighted "
+                      f"by each scene's point count, {threads} threads, {cpu_info()}"}
 
 
 # ---------------------------------------------------------------- 3D workload
