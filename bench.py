@@ -940,6 +940,7 @@ def main():
         line["cpu_baseline"] = {"value": m * NWALKS / tcpu, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{m} of {n} points x {NWALKS} walks (forward + adjoint), "
                                           f"{threads} threads, {cpu_info()}"}
+        line["accuracy"] = fp64_accuracy(scene, V, F, g, P, P_d, threads)
         # roofline of the adjoint kernel on the reference algorithm's work
         ref = reference_work(S, prm, adjp, P)
         samples = n * NWALKS
@@ -962,6 +963,29 @@ def main():
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def fp64_accuracy(scene, V, F, g, P, P_d, threads, npts=256, ref_walks=16384):
+    """Error of the solve against an FP64 solution.  The star with f = 1 has
+    no closed form, so the reference is the oracle's double-precision
+    walk-on-spheres (source term by its expectation R^2 / 4 per step) at
+    ref_walks walks on npts points spread over the grid; the GPU solve runs at
+    the bench's walk count on the same points.  RMSE ~ sqrt(SE_gpu^2 +
+    SE_ref^2) when both are unbiased."""
+    import torch
+    from oracle import oracle as O
+    idx = np.linspace(0, len(P) - 1, npts).astype(np.int64)
+    S = O.OracleScene(V, F, g)
+    ref_mean, ref_var, ref_trunc = S.solve_f64(P[idx], ref_walks, 1.0, eps=EPS, seed=424242, nthreads=threads)
+    mean, var = scene.solve(P_d[torch.as_tensor(idx, device=P_d.device)], walk_settings(11), want_var=True)
+    mean, var = mean.cpu().numpy(), var.cpu().numpy()
+    se = float(np.sqrt((var / NWALKS).mean()))
+    se_ref = float(np.sqrt((ref_var / ref_walks).mean()))
+    return {"rmse_vs_fp64": float(np.sqrt(((mean - ref_mean) ** 2).mean())), "rms_standard_error": se,
+            "expected_rmse": float(np.hypot(se, se_ref)),
+            "fp64_reference": {"points": npts, "walks": ref_walks, "rms_standard_error": se_ref,
+                               "truncated_walks": ref_trunc,
+                               "estimator": "oracle FP64 walk-on-spheres, source term R^2/4 per step"}}
 
 
 def walk_steps(steps, nsteps):

@@ -96,6 +96,7 @@ def lib() -> ctypes.CDLL:
         L.orc_bvh_counts.argtypes = [P, P, I, P, P, I]
         L.orc_inscribed_ball.argtypes = [P, P, P, P, I, ctypes.c_float, I, P, I]
         L.orc_walk_values.argtypes = [P, P, I, ctypes.POINTER(Params), P, P, P, I]
+        L.orc_solve_f64_2d.argtypes = [P, P, I, I, I, ctypes.c_double, ctypes.c_double, ctypes.c_uint64, I, P, P, P]
         L.orc_walk_records.argtypes = [P, P, I, ctypes.POINTER(Params), P, P, P, P, P, P, I]
         L.orc_reduce.argtypes = [P, I, I, P, P]
         L.orc_normal_derivative.argtypes = [P, P, P, P, P, P, I, ctypes.POINTER(Params), ctypes.POINTER(AdjParams),
@@ -187,6 +188,21 @@ class OracleScene:
         lib().orc_inscribed_ball(self.h, _p(pt), _p(nrm), _p(valid), valid.shape[0], eps, int(use_bvh), _p(R),
                                  nthreads)
         return R
+
+    def solve_f64(self, P, nwalks, fconst=0.0, eps=1e-3, max_steps=100_000, seed=0, nthreads=0):
+        """FP64 reference solution of -lap u = fconst with this scene's g (2D):
+        per-point mean and variance over `nwalks` double-precision walks whose
+        source term is its expectation f R^2 / 4 per step.  Returns (mean,
+        var, truncated walk count)."""
+        assert self.dim == 2
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        n = P.shape[0]
+        mean = np.zeros(n, np.float64)
+        var = np.zeros(n, np.float64)
+        tr = ctypes.c_longlong(0)
+        lib().orc_solve_f64_2d(self.h, _p(P), n, int(nwalks), int(max_steps), float(eps), float(fconst),
+                               int(seed) & 0xFFFFFFFFFFFFFFFF, nthreads, _p(mean), _p(var), ctypes.byref(tr))
+        return mean, var, int(tr.value)
 
     def walk_values(self, P, params: Params, nthreads=0):
         P = _f32(P)

@@ -1207,6 +1207,131 @@ void orc_soft_walk(void *s, const float *P, int n, const Params *prm, float *val
     }
 }
 
+// FP64 reference solution of -lap u = f (f constant) with Dirichlet data g
+// on a 2D polyline scene, for scoring the FP32 solvers against an FP64
+// solution where no closed form exists (the star with f = 1).  The walk of
+// include/wos.cuh:97-145 in double precision: nearest distance to the float
+// geometry (exact in double) through the LBVH, whose float boxes bound the
+// float segments exactly; a uniform direction on the circle from 53 random
+// bits; termination in the eps-shell with g interpolated at the closest
+// point.  Each step's source term is its expectation, f R^2 / 4 (the integral
+// over the disk of its Green's function log(R / r) / 2 pi), so the estimator
+// is unbiased for the same problem and samples no source point.  A walk still
+// inside after max_steps steps takes the value at its closest boundary point
+// (counted in *truncated).  Random numbers: Philox role 6, independent of the
+// FP32 walks.  Per-point mean and unbiased variance.
+static double seg_d2_f64(const Scene &S, int f, const double *p, double *h_out) {
+    const int *I = &S.F[(size_t)f * 2];
+    const double a[2] = {S.V[2 * I[0]], S.V[2 * I[0] + 1]}, b[2] = {S.V[2 * I[1]], S.V[2 * I[1] + 1]};
+    const double ba[2] = {b[0] - a[0], b[1] - a[1]}, pa[2] = {p[0] - a[0], p[1] - a[1]};
+    const double len2 = ba[0] * ba[0] + ba[1] * ba[1];
+    double h = len2 > 0.0 ? (pa[0] * ba[0] + pa[1] * ba[1]) / len2 : 0.0;
+    h = std::min(std::max(h, 0.0), 1.0);
+    const double v[2] = {pa[0] - h * ba[0], pa[1] - h * ba[1]};
+    *h_out = h;
+    return v[0] * v[0] + v[1] * v[1];
+}
+
+static inline double box_d2_f64(const float *lo, const float *hi, const double *p) {
+    double s = 0.0;
+    for (int k = 0; k < 2; ++k) {
+        const double d = std::max(std::max((double)lo[k] - p[k], p[k] - (double)hi[k]), 0.0);
+        s += d * d;
+    }
+    return s;
+}
+
+static int nearest_f64(const Scene &S, const double *p, double &best, double &hbest) {
+    int prim = -1;
+    best = std::numeric_limits<double>::infinity();
+    auto test = [&](int f) {
+        double h;
+        const double d2 = seg_d2_f64(S, f, p, &h);
+        if (d2 < best) {
+            best = d2;
+            hbest = h;
+            prim = f;
+        }
+    };
+    if (S.nF == 1) {
+        test(0);
+        return prim;
+    }
+    int stn[96];
+    double std2[96];
+    int sp = 0;
+    stn[sp] = 0;
+    std2[sp++] = 0.0;
+    while (sp > 0) {
+        --sp;
+        if (std2[sp] > best) continue;
+        const Node &nd = S.nodes[stn[sp]];
+        const double bd[2] = {box_d2_f64(nd.lo[0], nd.hi[0], p), box_d2_f64(nd.lo[1], nd.hi[1], p)};
+        const int nr = bd[1] < bd[0] ? 1 : 0, fr = 1 - nr;
+        const int order[2] = {fr, nr};  // push the far child first
+        for (int c : order) {
+            if (bd[c] > best) continue;
+            const int ch = nd.child[c];
+            if (ch < 0) {
+                test((int)(uint32_t)S.keys[~ch]);
+            } else if (sp < 96) {
+                stn[sp] = ch;
+                std2[sp++] = bd[c];
+            }
+        }
+    }
+    return prim;
+}
+
+static inline double g_f64(const Scene &S, int f, double h) {
+    const int *I = &S.F[(size_t)f * 2];
+    return (1.0 - h) * (double)S.g[I[0]] + h * (double)S.g[I[1]];
+}
+
+void orc_solve_f64_2d(void *s, const double *P, int n, int nwalks, int max_steps, double eps, double fconst,
+                      uint64_t seed, int nthreads, double *mean, double *var, long long *truncated) {
+    Scene *S = (Scene *)s;
+    const Rng rng = make_rng(seed);
+    const double two_pi = 6.283185307179586476925286766559;
+    long long trunc = 0;
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : trunc)
+    for (int i = 0; i < n; ++i) {
+        double sum = 0.0, sum2 = 0.0;
+        for (int w = 0; w < nwalks; ++w) {
+            double x[2] = {P[2 * i], P[2 * i + 1]}, acc = 0.0, val = 0.0, d2, h;
+            bool done = false;
+            for (int k = 0; k < max_steps && !done; ++k) {
+                const int f = nearest_f64(*S, x, d2, h);
+                const double d = std::sqrt(d2);
+                if (f < 0) {
+                    done = true;  // no geometry: scored 0
+                } else if (d < eps) {
+                    val = g_f64(*S, f, h) + acc;
+                    done = true;
+                } else {
+                    acc += fconst * d2 * 0.25;
+                    const U4 r = rng.draw((uint32_t)i, (uint32_t)w, (uint32_t)k, 6u);
+                    const double u = (double)(((uint64_t)r.x << 21) ^ (uint64_t)(r.y >> 11)) * 0x1p-53;
+                    x[0] += d * std::cos(two_pi * u);
+                    x[1] += d * std::sin(two_pi * u);
+                }
+            }
+            if (!done) {
+                const int f = nearest_f64(*S, x, d2, h);
+                val = (f >= 0 ? g_f64(*S, f, h) : 0.0) + acc;
+                ++trunc;
+            }
+            sum += val;
+            sum2 += val * val;
+        }
+        const double m = sum / nwalks;
+        mean[i] = m;
+        var[i] = nwalks > 1 ? std::max(0.0, (sum2 - nwalks * m * m) / (nwalks - 1)) : 0.0;
+    }
+    if (truncated) *truncated = trunc;
+}
+
 // Per-walk values for points x walks; vals[i * nwalks + w].
 void orc_walk_values(void *s, const float *P, int n, const Params *prm, float *vals, unsigned char *valid,
                      int *steps, int nthreads) {

@@ -87,6 +87,24 @@ def test_oracle_poisson_constant_source_disk(oracle):
         assert np.all(np.abs(mean - exact) < 4.5 * se + 2e-3), (use_IS, mean, exact, se)
 
 
+def test_oracle_fp64_reference_solution(oracle):
+    """The FP64 reference solver (used where no closed form exists): unbiased
+    on the circle for the harmonic x^3 - 3xy^2 (f = 0) and for u = (1 - r^2)/4
+    (g = 0, f = 1, source term by its expectation R^2 / 4 per step)."""
+    from wos import shapes
+    P = np.array([[0.0, 0.0], [0.3, -0.2], [-0.5, 0.4], [0.7, 0.1], [0.1, 0.85]])
+    S = _circle_oracle(oracle)
+    mean, var, trunc = S.solve_f64(P, 8192, 0.0, seed=1)
+    se = np.sqrt(var / 8192)
+    assert trunc == 0
+    assert np.all(np.abs(mean - shapes.harmonic_c1(P)) < 4.0 * se + 2e-3), (mean, se)
+    S0 = _circle_oracle(oracle, g_fn=lambda V: np.zeros(len(V)))
+    mean, var, trunc = S0.solve_f64(P, 8192, 1.0, seed=2)
+    se = np.sqrt(var / 8192)
+    exact = (1 - (P ** 2).sum(1)) / 4
+    assert np.all(np.abs(mean - exact) < 4.0 * se + 1e-3), (mean, exact, se)
+
+
 def test_oracle_poisson_sinusoid_source(oracle):
     """u = sin(3x + 4y) solves -Lap u = 25 sin(3x + 4y) (source type 2)."""
     from wos import shapes
