@@ -681,17 +681,66 @@ def c1_main(args):
     return 0
 
 
+def fd_check(make_scene, V, P_d, settings, adjoint, seeds, nvert=32, hs=(1e-3, 5e-4)):
+    """Vertex gradient of loss = mean(u^2) from the fused forward + adjoint
+    step against central finite differences with common random numbers (the
+    same seed on both sides), along seeded random directions at `nvert`
+    seeded random vertices, over `seeds` seeds; per vertex and step h the
+    z-score of (adjoint - FD) against the seed-to-seed standard errors of
+    both."""
+    import torch
+    dim = V.shape[1]
+    rng = np.random.default_rng(1)
+    ks = rng.choice(len(V), nvert, replace=False)
+    dirs = rng.normal(size=(nvert, dim))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    base, moved = make_scene(), make_scene()
+    adj = np.zeros((seeds, nvert))
+    fd = np.zeros((len(hs), seeds, nvert))
+    t0 = time.perf_counter()
+    for si in range(seeds):
+        s = settings(500 + si)
+        adj[si] = (base.solve_adjoint(P_d, s, adjoint, loss_kind=1)["dV"].cpu().numpy()[ks] * dirs).sum(1)
+        for j, (k, d) in enumerate(zip(ks, dirs)):
+            for hi, h in enumerate(hs):
+                loss = []
+                for sign in (1.0, -1.0):
+                    Vm = V.copy()
+                    Vm[k] += sign * h * d
+                    moved.update_vertices(torch.as_tensor(Vm, device=P_d.device))
+                    loss.append(float((moved.solve(P_d, s) ** 2).mean()))
+                fd[hi, si, j] = (loss[0] - loss[1]) / (2 * h)
+    t = time.perf_counter() - t0
+    checks = {}
+    for hi, h in enumerate(hs):
+        se = np.sqrt(adj.var(0, ddof=1) / seeds + fd[hi].var(0, ddof=1) / seeds)
+        z = (adj.mean(0) - fd[hi].mean(0)) / np.maximum(se, 1e-30)
+        checks[f"h{h:g}"] = {"within_2se": float(np.mean(np.abs(z) < 2.0)), "max_abs_z": float(np.abs(z).max()),
+                             "z": [float(x) for x in z], "fd_mean": [float(x) for x in fd[hi].mean(0)],
+                             "se": [float(x) for x in se]}
+    return t, {"vertices": [int(k) for k in ks], "adjoint_mean": [float(x) for x in adj.mean(0)],
+               "checks": checks}
+
+
+def fd_line(workload, npts, seeds, t, res, note):
+    return {
+        "metric": "vertex_gradient_fd_check", "value": res["checks"]["h0.001"]["within_2se"],
+        "unit": "fraction of vertices within 2 SE (h = 1e-3)", "n_gpus": 1, "steps": seeds, "warmup": 0,
+        "ms_per_step": t / seeds * 1e3, "higher_is_better": True, "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": workload, "points": npts, "points_note": note, "h": [1e-3, 5e-4], "seeds": seeds,
+                   "fd": "central, common random numbers"},
+        **res,
+    }
+
+
 def fd_main(args):
-    """The 2D differentiable solve's gradient check: the vertex gradient of
-    loss = mean(u^2) from the fused forward + adjoint step against central
-    finite differences (h = 1e-3 as specified, and h = 5e-4; common random
-    numbers: the same seed on both sides) along seeded random directions at
-    32 seeded random vertices, over `--seeds` seeds; per vertex the z-score
-    of (adjoint - FD) against the seed-to-seed standard errors of both.  With
-    h equal to the termination shell epsilon (1e-3), a move changes which
-    walks end in the shell, so where the normal derivative is large the loss
-    is visibly nonlinear at that scale and the h = 1e-3 difference is biased;
-    h = 5e-4 shows the estimate converging to the adjoint.  Query points within 0.01 of the
+    """The 2D differentiable solve's gradient check (fd_check) at 32 vertices,
+    h = 1e-3 as specified and h = 5e-4.  With h equal to the termination
+    shell epsilon (1e-3), a move changes which walks end in the shell, so
+    where the normal derivative is large the loss is visibly nonlinear at
+    that scale and the h = 1e-3 difference is biased; h = 5e-4 shows the
+    estimate converging to the adjoint.  Query points within 0.01 of the
     boundary are left out: a vertex moved by h can carry such a point outside
     the domain, which ends its walks (value 0) -- a jump of the loss that the
     finite difference sees and the shape derivative of the fixed point set
@@ -704,48 +753,35 @@ def fd_main(args):
     dev = torch.device("cuda", local)
     V, F, g, P = make_workload()
     P = np.ascontiguousarray(P[shapes.inside_star(P, STAR["r0"], STAR["amp"], STAR["lobes"], margin=0.01)])
-    P_d = torch.as_tensor(P, device=dev)
-    rng = np.random.default_rng(1)
-    ks = rng.choice(len(V), 32, replace=False)
-    dirs = rng.normal(size=(32, 2))
-    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
-    hs = (1e-3, 5e-4)
-    base = NativeScene(V, F, g, 2, SOURCE)
-    moved = NativeScene(V, F, g, 2, SOURCE)
-    adj = np.zeros((args.seeds, 32))
-    fd = np.zeros((len(hs), args.seeds, 32))
-    t0 = time.perf_counter()
-    for si in range(args.seeds):
-        s = walk_settings(500 + si)
-        adj[si] = (base.solve_adjoint(P_d, s, adjoint_settings(), loss_kind=1)["dV"].cpu().numpy()[ks] * dirs).sum(1)
-        for j, (k, d) in enumerate(zip(ks, dirs)):
-            for hi, h in enumerate(hs):
-                loss = []
-                for sign in (1.0, -1.0):
-                    Vm = V.copy()
-                    Vm[k] += sign * h * d
-                    moved.update_vertices(torch.as_tensor(Vm, device=dev))
-                    loss.append(float((moved.solve(P_d, s) ** 2).mean()))
-                fd[hi, si, j] = (loss[0] - loss[1]) / (2 * h)
-    t = time.perf_counter() - t0
-    checks = {}
-    for hi, h in enumerate(hs):
-        se = np.sqrt(adj.var(0, ddof=1) / args.seeds + fd[hi].var(0, ddof=1) / args.seeds)
-        z = (adj.mean(0) - fd[hi].mean(0)) / np.maximum(se, 1e-30)
-        checks[f"h{h:g}"] = {"within_2se": float(np.mean(np.abs(z) < 2.0)), "max_abs_z": float(np.abs(z).max()),
-                             "z": [float(x) for x in z], "fd_mean": [float(x) for x in fd[hi].mean(0)],
-                             "se": [float(x) for x in se]}
-    line = {
-        "metric": "vertex_gradient_fd_check", "value": checks["h0.001"]["within_2se"],
-        "unit": "fraction of vertices within 2 SE (h = 1e-3)", "n_gpus": 1, "steps": args.seeds, "warmup": 0,
-        "ms_per_step": t / args.seeds * 1e3, "higher_is_better": True, "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic",
-        "config": {"workload": workload_config(len(P))["workload"], "points": len(P),
-                   "points_note": "grid points at least 0.01 inside the boundary", "vertices": 32, "h": list(hs),
-                   "seeds": args.seeds, "fd": "central, common random numbers"},
-        "adjoint_mean": [float(x) for x in adj.mean(0)], "checks": checks,
-    }
-    print(json.dumps(line), flush=True)
+    t, res = fd_check(lambda: NativeScene(V, F, g, 2, SOURCE), V, torch.as_tensor(P, device=dev), walk_settings,
+                      adjoint_settings(), args.seeds)
+    print(json.dumps(fd_line(workload_config(len(P))["workload"], len(P), args.seeds, t, res,
+                             "grid points at least 0.01 inside the boundary")), flush=True)
+    return 0
+
+
+def c3fd_main(args):
+    """The 3D solve's gradient check (fd_check) on the displaced icosphere
+    (81,920 triangles, g = x^2 - y^2 + z) at 32 vertices, 20,000 seeded
+    interior points at least 0.01 inside (radially), 128 walks, epsilon 1e-3."""
+    import torch
+    from wos import shapes
+    from wos.native import AdjointSettings, NativeScene, WalkSettings
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    V, F = shapes.displaced_icosphere(6, 0.15, seed=0)
+    g = shapes.harmonic_c3(V).astype(np.float32)
+    P = shapes.sample_interior_3d(20000, shapes.displaced_radius_fn(0.15, 0), seed=2, margin=0.01)
+    P = np.ascontiguousarray(P[:20000]).astype(np.float32)
+    adj = AdjointSettings(epsilon2=1e-3, clamping=0.1, want_dV=True, want_dg=True, want_dsrc=False)
+
+    def ws(seed):
+        return WalkSettings(nwalks=128, nsteps=64, epsilon=1e-3, seed=seed)
+
+    t, res = fd_check(lambda: NativeScene(V, F, g), V, torch.as_tensor(P, device=dev), ws, adj, args.seeds)
+    print(json.dumps(fd_line("3d_forward_adjoint_icosphere81920_pts20000_walks128", len(P), args.seeds, t, res,
+                             "seeded interior points at least 0.01 inside (radially)")), flush=True)
     return 0
 
 
@@ -819,9 +855,9 @@ def main():
     ap.add_argument("--grid", type=int, default=GRID, help="query grid (smaller only for profiling captures)")
     ap.add_argument("--walks", type=int, default=None,
                     help="walks per point (c2: 256, c3: 128; smaller only for profiling)")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2fd", "c3", "c4", "batched"],
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2fd", "c3", "c3fd", "c4", "batched"],
                     help="c2: the 2D differentiable solve (default); c1: the plain 2D primal solve; "
-                         "c2fd: c2's vertex gradients against finite differences; "
+                         "c2fd / c3fd: vertex gradients against finite differences; "
                          "c3: the 3D forward + adjoint solve; c4: the 2D inverse problem; "
                          "batched: many scenes in one launch")
     ap.add_argument("--seeds", type=int, default=16, help="seeds of the c2fd gradient check")
@@ -836,6 +872,8 @@ def main():
         return c1_main(args)
     if args.workload == "c2fd" and args.impl == "ours":
         return fd_main(args)
+    if args.workload == "c3fd" and args.impl == "ours":
+        return c3fd_main(args)
     if args.workload == "c3" and args.impl == "ours":
         return c3_main(args)
     if args.workload == "c4" and args.impl == "ours":
