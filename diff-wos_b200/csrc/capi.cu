@@ -236,6 +236,16 @@ int wos_closest_point(wos_scene_t scene, const float *P, int n, int use_bvh, int
     return launch_closest(scene->impl, P, n, use_bvh != 0, o, (cudaStream_t)stream);
 }
 
+int wos_sdf(wos_scene_t scene, const float *P, int n, int use_bvh, float *sdf, wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (n < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "n must be >= 0");
+    if (n == 0) return 0;
+    WOS_CHECK_DEV(P, "P");
+    WOS_CHECK_DEV(sdf, "sdf");
+    QueryOut o{nullptr, nullptr, nullptr, nullptr, nullptr, sdf, nullptr};
+    return launch_closest(scene->impl, P, n, use_bvh != 0, o, (cudaStream_t)stream);
+}
+
 int wos_largest_inscribed_ball(wos_scene_t scene, const uint8_t *valid, const float *pt, const float *normal, int n,
                                float epsilon, int use_bvh, float *R, wos_stream_t stream) {
     if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");

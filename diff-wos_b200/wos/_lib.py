@@ -128,6 +128,7 @@ SIGNATURES = {
     "wos_scene_get_info": (_I, [_P, ctypes.POINTER(WosSceneInfo)]),
     "wos_scene_get_normals": (_I, [_P, _P, _P]),
     "wos_closest_point": (_I, [_P, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "wos_sdf": (_I, [_P, _P, _I, _I, _P, _P]),
     "wos_largest_inscribed_ball": (_I, [_P, _P, _P, _P, _I, _F, _I, _P, _P]),
     "wos_walk_records": (_I, [_P, _P, _I, ctypes.POINTER(WosParams), _P, _P, _P, _P, _P, _P, _P]),
     "wos_walk_values": (_I, [_P, _P, _I, ctypes.POINTER(WosParams), _P, _P, _P]),

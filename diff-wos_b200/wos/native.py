@@ -167,6 +167,15 @@ class NativeScene:
                  _ptr(out.get("sdf")), _ptr(out.get("inside")), stream())
         return out
 
+    def sdf(self, P, use_bvh=True) -> torch.Tensor:
+        """Signed distance to the boundary, negative inside (wos_sdf)."""
+        P = as_cuda(P, torch.float32, self.dim)
+        n = int(P.shape[0])
+        out = torch.empty(n, dtype=torch.float32, device=self.device)
+        if n:
+            call("wos_sdf", self.h, P.data_ptr(), n, int(use_bvh), out.data_ptr(), stream())
+        return out
+
     def inscribed_ball(self, valid, pt, nrm, epsilon=1e-3, use_bvh=True) -> torch.Tensor:
         valid = as_cuda(valid, torch.uint8).reshape(-1)
         pt = as_cuda(pt, torch.float32, self.dim)

@@ -194,7 +194,7 @@ class Polyline:
         return its
 
     def sdf(self, p) -> torch.Tensor:
-        return self._native.closest(points(p, self.dim), self.use_bvh, want=("sdf",))["sdf"]
+        return self._native.sdf(points(p, self.dim), self.use_bvh)
 
     def is_inside(self, p) -> torch.Tensor:
         return self._native.closest(points(p, self.dim), self.use_bvh, want=("inside",))["inside"].bool()

@@ -148,7 +148,7 @@ class Scene3D:
         return its
 
     def sdf(self, p, active=None) -> torch.Tensor:
-        return self._native.closest(points(p, 3), self.use_bvh, want=("sdf",))["sdf"]
+        return self._native.sdf(points(p, 3), self.use_bvh)
 
     def is_inside(self, p) -> torch.Tensor:
         return self._native.closest(points(p, 3), self.use_bvh, want=("inside",))["inside"].bool()

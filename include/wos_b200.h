@@ -175,6 +175,11 @@ WOS_API int wos_scene_get_normals(wos_scene_t scene, float *out, wos_stream_t st
 WOS_API int wos_closest_point(wos_scene_t scene, const float *P, int n, int use_bvh, int32_t *prim, float *dist,
                       float *t_or_uv, float *pt, float *normal, float *sdf, uint8_t *inside, wos_stream_t stream);
 
+/* Scene.sdf (include/scene.cuh:148-178): signed distance of n points P
+ * (n x dim) to the boundary, negative inside; the sdf output of
+ * wos_closest_point alone. */
+WOS_API int wos_sdf(wos_scene_t scene, const float *P, int n, int use_bvh, float *sdf, wos_stream_t stream);
+
 /* Scene.largest_inscribed_ball(its, epsilon) (include/scene.cuh:225-249,
  * :659-704): 10-step bisection of the ball tangent at boundary point pt with
  * inward normal `normal`; R = 0 where valid == 0. */

@@ -67,6 +67,7 @@ def test_argument_validation_without_gpu():
         _lib.WOS_ERR_INVALID_ARGUMENT
     assert b"nwalks" in L.wos_last_error_string()
     assert L.wos_solve_workspace_size(10, ctypes.byref(_lib.WosParams(4, 32, 1e-3))) >= 10 * 4 * 4
+    assert L.wos_sdf(None, None, 1, 1, None, None) == _lib.WOS_ERR_INVALID_ARGUMENT
     bt = (ctypes.c_int32 * 1)(100)
     ch = (ctypes.c_int32 * 1)(16)
     assert L.wos_batch_autotune(None, bt, ch, 1, 1, None, None, None) == _lib.WOS_ERR_INVALID_ARGUMENT

@@ -83,6 +83,7 @@ def test_closest_point_bit_exact(cuda, oracle, kind, use_bvh):
     assert np.array_equal(_np(o["n"]), r["n"])
     assert np.array_equal(_np(o["sdf"]), r["sdf"])
     assert np.array_equal(_np(o["inside"]), r["inside"])
+    assert np.array_equal(_np(ns.sdf(P, use_bvh)), r["sdf"])  # wos_sdf
 
 
 def test_bvh_equals_brute_force_ties(cuda, oracle):
