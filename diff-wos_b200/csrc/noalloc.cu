@@ -12,10 +12,10 @@
 //
 // The array costs every GPU that loads the library 16 MiB + 256 bytes until
 // the process exits.  Its device address is looked up (cudaGetSymbolAddress)
-// on the first call on each device, with that device current.  All calls
+// on every call, with the caller's device current: the lookup is a host-side
+// table read, and a fresh lookup stays valid across a device reset or a
+// re-created primary context, where a cached address would dangle.  All calls
 // share the one array: calls that overlap on the GPU race on it.
-#include <mutex>
-
 #include "../../include/wos_b200.h"
 #include "scene_impl.h"
 #include "walk.h"
@@ -28,26 +28,14 @@ constexpr size_t NOALLOC_BYTES = NOALLOC_COUNTER_BYTES + (size_t)WOS_NOALLOC_MAX
 // [queue counter (256 B)][per-walk values (WOS_NOALLOC_MAX_WALKS floats)]
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 
-constexpr int NOALLOC_MAX_DEVICES = 256;
-static std::mutex g_noalloc_mu;
-static void *g_noalloc_addr[NOALLOC_MAX_DEVICES];
-
 // Device address of the array on the current device.  In host code the
 // symbol g_noalloc_scratch is only a host-side stand-in, so kernels are given
 // this address, never the symbol.
 static int noalloc_scratch(char **out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return fail_cuda(e, "cudaGetDevice");
-    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(WOS_ERR_UNSUPPORTED, "device index out of range");
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (g_noalloc_addr[dev] == nullptr) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return fail_cuda(e, "cudaGetSymbolAddress(noalloc scratch)");
-        g_noalloc_addr[dev] = p;
-    }
-    *out = static_cast<char *>(g_noalloc_addr[dev]);
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaGetSymbolAddress(noalloc scratch)");
+    *out = static_cast<char *>(p);
     return 0;
 }
 

@@ -76,6 +76,20 @@ def sharded_adjoint(native_scene, P, settings, adjoint, dLdu):
     if count > 0:
         dV, dg, ds = native_scene.adjoint(P, local, adjoint, dLdu * (count / settings.nwalks))
     else:
-        dV, dg, ds = native_scene.adjoint(P, dataclasses.replace(settings, nwalks=1), adjoint, dLdu * 0.0)
+        # no walks on this rank (nwalks < world size): contribute exact zeros
+        # to the sum, without a launch whose inf/NaN walks would turn 0 * inf
+        # into NaN on every rank
+        dV, dg, ds = _zero_gradients(native_scene, adjoint, P.device)
     allreduce_sum_([dV, dg, ds])
+    return dV, dg, ds
+
+
+def _zero_gradients(native_scene, adjoint, device):
+    """Zero dV (nV x dim), dg (nV) and dsrc (5) as the native adjoint returns
+    them, None where the matching want_* flag is off."""
+    nV, dim = int(native_scene.nV), int(native_scene.dim)
+    f32 = torch.float32
+    dV = torch.zeros((nV, dim), dtype=f32, device=device) if adjoint.want_dV else None
+    dg = torch.zeros(nV, dtype=f32, device=device) if adjoint.want_dg else None
+    ds = torch.zeros(5, dtype=f32, device=device) if adjoint.want_dsrc else None
     return dV, dg, ds

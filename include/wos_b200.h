@@ -422,9 +422,11 @@ WOS_API int wos_batch_destroy(wos_batch_t b, wos_stream_t stream);
  * Scratch is a fixed array inside the library: 16 MiB + 256 bytes on every
  * GPU that loads it, held until the process exits.  n * nwalks must not
  * exceed WOS_NOALLOC_MAX_WALKS; larger requests fail with WOS_ERR_WORKSPACE
- * and a message (split the points, or use wos_solve).  The first call on a
- * device looks up the array's device address with that device current; make
- * that first call before any stream capture.  All calls share the one
+ * and a message (split the points, or use wos_solve).  Every call looks up
+ * the array's device address with the caller's device current (so a device
+ * reset between calls is harmless); the first call on a device may also load
+ * the library's device code there, so make that first call before any stream
+ * capture.  All calls share the one
  * array, so calls that overlap on the GPU (concurrent streams or threads)
  * race on it: order them on one stream.  Results equal wos_solve's. */
 WOS_API int wos_solve_noalloc(wos_scene_t scene, const float *P, int n, const wos_params *p, double *mean, double *var,

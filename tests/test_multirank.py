@@ -39,15 +39,20 @@ class FakeNative:
 
     def adjoint(self, P, s, a, dLdu):
         n = P.shape[0]
-        dV = torch.zeros(self.nV, self.dim, dtype=torch.float32)
-        dg = torch.zeros(self.nV, dtype=torch.float32)
-        ds = torch.zeros(5, dtype=torch.float32)
+        dV = torch.zeros(self.nV, self.dim, dtype=torch.float32) if a.want_dV else None
+        dg = torch.zeros(self.nV, dtype=torch.float32) if a.want_dg else None
+        ds = torch.zeros(5, dtype=torch.float32) if a.want_dsrc else None
+        if s.nwalks < 1:
+            raise AssertionError("the sharded adjoint must not launch a rank without walks")
         for i in range(n):
             for k in range(s.walk_offset, s.walk_offset + s.nwalks):
                 W = float(dLdu[i]) / s.nwalks
-                dV[(i + k) % self.nV] += W * torch.tensor([1.0, float(k)])
-                dg[k % self.nV] += W
-                ds[i % 5] += W * k
+                if dV is not None:
+                    dV[(i + k) % self.nV] += W * torch.tensor([1.0, float(k)])
+                if dg is not None:
+                    dg[k % self.nV] += W
+                if ds is not None:
+                    ds[i % 5] += W * k
         return dV, dg, ds
 
 
@@ -59,7 +64,7 @@ def _free_port():
     return p
 
 
-def _worker(rank, size, port, out):
+def _worker(rank, size, port, out, nwalks=11):
     sys.path.insert(0, str(ROOT / "diff-wos_b200"))
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     import torch.distributed as dist
@@ -68,11 +73,11 @@ def _worker(rank, size, port, out):
     dist.init_process_group("gloo", rank=rank, world_size=size)
     try:
         P = torch.zeros(7, 2)
-        s = WalkSettings(nwalks=11, walk_offset=3, seed=1)
+        s = WalkSettings(nwalks=nwalks, walk_offset=3, seed=1)
         fake = FakeNative()
         mean = wdist.sharded_solve(fake, P, s)
         dLdu = torch.linspace(-1.0, 2.0, 7)
-        dV, dg, ds = wdist.sharded_adjoint(fake, P, s, AdjointSettings(), dLdu)
+        dV, dg, ds = wdist.sharded_adjoint(fake, P, s, AdjointSettings(want_dg=True, want_dsrc=True), dLdu)
         t = torch.tensor([float(rank + 1)])
         mx = wdist.max_over_ranks(3.0 * (rank + 1))
         out[rank] = (mean.numpy(), dV.numpy(), dg.numpy(), ds.numpy(), mx)
@@ -92,12 +97,14 @@ def test_shard_partition():
 
 
 @pytest.mark.timeout(120)
-def test_two_rank_gloo_matches_single_rank():
+@pytest.mark.parametrize("nwalks", [11, 1])
+def test_two_rank_gloo_matches_single_rank(nwalks):
+    """nwalks = 1 leaves rank 1 without walks: it must add zeros, not launch."""
     ctx = mp.get_context("spawn")
     mgr = ctx.Manager()
     out = mgr.dict()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, out)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, out, nwalks)) for r in range(2)]
     for p in procs:
         p.start()
     for p in procs:
@@ -107,9 +114,9 @@ def test_two_rank_gloo_matches_single_rank():
     from wos.native import AdjointSettings, WalkSettings
     fake = FakeNative()
     P = torch.zeros(7, 2)
-    s = WalkSettings(nwalks=11, walk_offset=3, seed=1)
+    s = WalkSettings(nwalks=nwalks, walk_offset=3, seed=1)
     ref_mean = fake.solve(P, s).numpy()
-    ref = fake.adjoint(P, s, AdjointSettings(), torch.linspace(-1.0, 2.0, 7))
+    ref = fake.adjoint(P, s, AdjointSettings(want_dg=True, want_dsrc=True), torch.linspace(-1.0, 2.0, 7))
     for r in range(2):
         mean, dV, dg, ds, mx = out[r]
         np.testing.assert_allclose(mean, ref_mean, rtol=1e-12)
