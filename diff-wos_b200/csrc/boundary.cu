@@ -41,6 +41,7 @@ struct DetectorCfg {
     int au, av, slab;
     float slab_c, slab_h;
     float size;
+    double pdf_scale;  // 1 / pdf = total measure * pdf_scale
 };
 
 // A sample's primitive (from the inclusive prefix sums `cdf` of the
@@ -116,8 +117,8 @@ __global__ void k_boundary(const float *__restrict__ V, const int *__restrict__ 
         if (det.slab >= 0) ok = ok && fabsf(x[det.slab] - det.slab_c) < det.slab_h;
         const long long idx = (long long)iu + (long long)(det.res[1] - iv) * det.res[0];
         if (!ok || idx < 0 || idx >= npix) continue;
-        // -val / pdf / (size * nwalks), pdf = 1 / total measure
-        const double w = -(double)val * total / ((double)det.size * nwalks);
+        // -val / pdf / (size * nwalks), pdf = 1 / (total measure * pdf_scale)
+        const double w = -(double)val * total * det.pdf_scale / ((double)det.size * nwalks);
         if (tV != nullptr && img_tan != nullptr) {
             double nd = 0.0;
             for (int j = 0; j < D; ++j)
@@ -163,6 +164,8 @@ int launch_boundary(const SceneImpl &S, const wos_detector &d, int nwalks, uint6
         c.slab_c = d.slab_center;
         c.slab_h = d.slab_half_width;
         c.size = d.size;
+        // the reference's 3D pdf divides by |ab x ac| = 2 * area (wos/scene3d.py:262)
+        c.pdf_scale = (S.dim == 3 && (d.flags & WOS_DETECTOR_REFERENCE_AREA_PDF)) ? 2.0 : 1.0;
         const long long ns = (long long)d.res[0] * d.res[1] * nwalks;
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);

@@ -623,6 +623,8 @@ int wos_boundary_term(wos_scene_t scene, const wos_detector *det, int nwalks, ui
         det->slab_axis < -1 || det->slab_axis >= S.dim)
         return fail(WOS_ERR_INVALID_ARGUMENT, "detector axes out of range for the scene's dimension");
     if (!(det->size > 0.0f)) return fail(WOS_ERR_INVALID_ARGUMENT, "detector size must be > 0");
+    if ((det->flags & ~WOS_DETECTOR_REFERENCE_AREA_PDF) != 0)
+        return fail(WOS_ERR_INVALID_ARGUMENT, "unknown detector flags");
     if ((dV_dir == nullptr) != (image_tangent == nullptr))
         return fail(WOS_ERR_INVALID_ARGUMENT, "dV_dir and image_tangent go together");
     if ((dLdI == nullptr) != (dV == nullptr)) return fail(WOS_ERR_INVALID_ARGUMENT, "dLdI and dV go together");

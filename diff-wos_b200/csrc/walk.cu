@@ -14,9 +14,9 @@
 //
 // Reference functions restated: WoSDevice<N>::walk (include/wos.cuh:97-145),
 // WoS<N>::solve / singleWalk launchers (:184-448), normal_derivative
-// (wos/wos.py:184-232, wos/wos_with_source.py:154-232, wos/wos3d.py:248-286),
-// tangent_derivative (wos/scene.py:451-460, wos/wos3d.py:288-307), OursCUDA /
-// Ours3D (wos/wos_grad.py:130-151, wos/wos_grad_3d.py:391-411).
+// (wos/wos.py:59-107, wos/wos_with_source.py:154-232, wos/wos3d.py:97-135),
+// tangent_derivative (wos/scene.py:451-460, wos/wos3d.py:137-156), OursCUDA /
+// Ours3D (wos/wos_grad.py:130-151, wos/wos_grad_3d.py:117-137).
 #include <algorithm>
 
 #include "scene_impl.h"
@@ -534,7 +534,7 @@ __device__ __forceinline__ float eval_P(const float *c, const float *y, const fl
 }
 
 // State of one normal-derivative sample on the inscribed ball of radius R
-// centred at c = p + rn R (wos/wos.py:196-232, wos/wos3d.py:254-286).  The
+// centred at c = p + rn R (wos/wos.py:71-107, wos/wos3d.py:103-135).  The
 // outward normal n = -rn, the centre and the second tangent are recomputed
 // where needed (the same float operations as storing them), which keeps the
 // per-thread state small.
@@ -989,7 +989,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
             } else {
                 w.start(qpos, D);
                 w.last = hit.prim;
-                const int r = walker_advance<D>(w, S, hit, c, a.epsilon2, false, false, pt, wk, role, false, cdf);
+                const int r = walker_advance<D>(w, S, hit, c, a.epsilon2, c.project != 0, false, pt, wk, role, false, cdf);
                 if (r == W_CONTINUE) {
                     phase = PH_ANTI_WALK;
                     continue;
@@ -1002,7 +1002,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
                 finish_anti = true;
             }
         } else {  // PH_ANTI_WALK
-            const int r = walker_advance<D>(w, S, hit, c, a.epsilon2, false, false, pt, wk, role, false, cdf);
+            const int r = walker_advance<D>(w, S, hit, c, a.epsilon2, c.project != 0, false, pt, wk, role, false, cdf);
             if (r == W_CONTINUE) continue;
             if (r == W_VALID) {
                 const Rec r2 = closest_record<D>(S, w.p, hit.prim);
@@ -1980,7 +1980,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
             } else {
                 w.start(qpos, D);
                 w.last = hit.prim;
-                const int r = walker_advance<D>(w, S, hit, c, a.epsilon2, false, false, pt, wk, role, false, S.guide);
+                const int r = walker_advance<D>(w, S, hit, c, a.epsilon2, c.project != 0, false, pt, wk, role, false, S.guide);
                 if (r == W_CONTINUE) {
                     phase = PH_ANTI_WALK;
                     continue;
@@ -1993,7 +1993,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
                 finish_anti = true;
             }
         } else {  // PH_ANTI_WALK
-            const int r = walker_advance<D>(w, S, hit, c, a.epsilon2, false, false, pt, wk, role, false, S.guide);
+            const int r = walker_advance<D>(w, S, hit, c, a.epsilon2, c.project != 0, false, pt, wk, role, false, S.guide);
             if (r == W_CONTINUE) continue;
             if (r == W_VALID) {
                 const Rec r2 = closest_record<D>(S, w.p, hit.prim);

@@ -96,7 +96,11 @@ class WosDetector(ctypes.Structure):
         ("slab_center", ctypes.c_float),
         ("slab_half_width", ctypes.c_float),
         ("size", ctypes.c_float),
+        ("flags", ctypes.c_int32),
     ]
+
+
+WOS_DETECTOR_REFERENCE_AREA_PDF = 1
 
 
 class WosBatchItem(ctypes.Structure):

@@ -8,21 +8,31 @@ import numpy as np
 
 
 def _read(filename, elem: str, dim: int, flip_orientation: bool):
+    """Vertices (float64, first `dim` coordinates), element indices (int64,
+    0-based; for `l` lines the first two) and `c` values (float64), as the
+    reference's readers return them (wos/io.py:20-38, :54-71)."""
     V, I, C = [], [], []
     with open(filename, "r") as f:
         for line in f:
-            line = line.strip()
             if line.startswith("v "):
-                V.append([float(x) for x in line[2:].split()][:dim])
+                V.append([float(x) for x in line.split()[1:]][:dim])
             elif line.startswith(elem + " "):
-                idx = [int(x.split("/")[0]) - 1 for x in line[2:].split()]
+                idx = [int(x.split("/")[0]) - 1 for x in line.split()[1:]]
                 if flip_orientation:
                     idx = idx[::-1]
-                I.append(idx)
+                I.append(idx[:2] if elem == "l" else idx)
             elif line.startswith("c "):
-                C.append(float(line[2:].split()[0]))
-    return np.asarray(V, np.float32).reshape(-1, dim), np.asarray(I, np.int32).reshape(-1, dim), np.asarray(
-        C, np.float32)
+                C.append(float(line.split()[1]))
+    return (np.asarray(V, np.float64).reshape(-1, dim), np.asarray(I, np.int64).reshape(-1, dim),
+            np.asarray(C, np.float64))
+
+
+def normalize_vertices(V):
+    """Centre on the vertex mean and scale the farthest vertex to radius 1,
+    in double precision, then round to float32 (wos/scene.py:232-237)."""
+    V = np.asarray(V, np.float64)
+    V = V - V.mean(0)
+    return (V / np.linalg.norm(V, axis=1).max()).astype(np.float32)
 
 
 def read_2d_obj(filename, flip_orientation=False):

@@ -38,11 +38,11 @@ class Detector:
         dx, dy = self.pixel()
         return (dx, dy, 0.0)
 
-    def c(self):
-        """The detector for the C ABI (wos_detector)."""
+    def c(self, flags: int = 0):
+        """The detector for the C ABI (wos_detector); flags: WOS_DETECTOR_* bits."""
         from ._lib import WosDetector
         return WosDetector((ctypes.c_float * 2)(*self.vmin), (ctypes.c_float * 2)(*self.vmax),
-                           (ctypes.c_int32 * 2)(*self.res), 0, 1, -1, 0.0, 0.0, float(self.size()))
+                           (ctypes.c_int32 * 2)(*self.res), 0, 1, -1, 0.0, 0.0, float(self.size()), int(flags))
 
     def make_points(self) -> torch.Tensor:
         x = torch.linspace(self.vmin[0], self.vmax[0], self.res[0], device="cuda")
@@ -144,14 +144,14 @@ class Polyline:
 
     @staticmethod
     def from_obj(filename, normalize=True, flip_orientation=False, **kw):
-        from .io import read_2d_obj
+        """wos/scene.py:211-240: read an OBJ polyline (`v`, `l`, `c` lines),
+        centre it on the vertex mean and scale it to unit radius in double
+        precision.  A file without `c` lines gets zero values."""
+        from .io import normalize_vertices, read_2d_obj
         V, F, g = read_2d_obj(filename, flip_orientation=flip_orientation)
-        if normalize:
-            V = V - V.mean(0)
-            V = V / np.linalg.norm(V, axis=1).max()
-        if len(g) != len(V):
-            g = np.zeros(len(V), np.float32)
-        return Polyline(V.astype(np.float32), F, g, **kw)
+        V = normalize_vertices(V) if normalize else V.astype(np.float32)
+        g = g.astype(np.float32) if len(g) == len(V) else np.zeros(len(V), np.float32)
+        return Polyline(V, F.astype(np.int32), g, **kw)
 
     def update_values(self, values):
         """Replace the Dirichlet values (keeps the geometry and LBVH)."""

@@ -28,9 +28,9 @@ class Detector3D(Detector):
         z = torch.full((p.shape[0], 1), float(self.z), device=p.device)
         return torch.cat([p, z], 1).contiguous()
 
-    def c(self):
+    def c(self, flags: int = 0):
         """Slab |z - self.z| < l_z / 2 (wos/scene3d.py:35-41)."""
-        d = super().c()
+        d = super().c(flags)
         d.slab_axis, d.slab_center, d.slab_half_width = 2, float(self.z), float(self.l_z) / 2
         return d
 
@@ -58,9 +58,9 @@ class Detector3DY(Detector):
         """Slab volume (image area x l_y)."""
         return float(np.prod(np.subtract(self.vmax, self.vmin))) * self.l_y
 
-    def c(self):
+    def c(self, flags: int = 0):
         """Image axes x, z; slab |y - self.y| < l_y / 2 (wos/scene3d.py:73-81)."""
-        d = super().c()
+        d = super().c(flags)
         d.axis_u, d.axis_v = 0, 2
         d.slab_axis, d.slab_center, d.slab_half_width = 1, float(self.y), float(self.l_y) / 2
         return d
@@ -106,14 +106,17 @@ class Scene3D:
 
     @staticmethod
     def from_obj(filename, normalize=True, flip_orientation=False, **kw):
-        from .io import read_3d_obj
+        """OBJ triangle mesh (`v`, `f`, `c` lines), optionally centred and
+        scaled to unit radius in double precision.  The reference's
+        Scene3D.from_obj keeps only two coordinates per vertex
+        (wos/scene3d.py:127) and cannot build a 3D scene; this reads all three,
+        as its read_3d_obj does (wos/io.py:54-71).  A file without `c` lines
+        gets zero values."""
+        from .io import normalize_vertices, read_3d_obj
         V, F, g = read_3d_obj(filename, flip_orientation=flip_orientation)
-        if normalize:
-            V = V - V.mean(0)
-            V = V / np.linalg.norm(V, axis=1).max()
-        if len(g) != len(V):
-            g = np.zeros(len(V), np.float32)
-        return Scene3D(V.astype(np.float32), F, g, **kw)
+        V = normalize_vertices(V) if normalize else V.astype(np.float32)
+        g = g.astype(np.float32) if len(g) == len(V) else np.zeros(len(V), np.float32)
+        return Scene3D(V, F.astype(np.int32), g, **kw)
 
     def update_values(self, values):
         self.values = tensor(values, torch.float32).reshape(-1)
@@ -179,7 +182,7 @@ class Scene3D:
         return ClosestPointRecord3D(valid=its.valid, p=p, n=its.n, uv=uv, val=val, prim_id=its.prim_id)
 
     def tangent_derivative(self, its: ClosestPointRecord3D):
-        """Tangential gradient from the face's value slope (wos/wos3d.py:288-307)."""
+        """Tangential gradient from the face's value slope (wos/wos3d.py:137-156)."""
         prim = its.prim_id.long().clamp_min(0)
         f = self.indices.long()[prim]
         V = self.vertices.detach()

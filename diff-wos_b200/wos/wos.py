@@ -26,7 +26,7 @@ class WoS(Solver):
     source_in_normal_derivative = False
 
     def normal_derivative(self, its, scene, sampler, override_R=None, clamping=1e-1, control_variates=True):
-        """du/dn at boundary records (wos/wos.py:184-232): off-centred Poisson
+        """du/dn at boundary records (wos/wos.py:59-107): off-centred Poisson
         kernel on the largest inscribed ball, two antithetic samples, each a
         full walk at this solver's epsilon.  Returns (grad * n_x, grad * n_y)
         with n the outward normal."""

@@ -17,7 +17,7 @@ class WoS3D(Solver):
     project_unterminated = True
 
     def normal_derivative(self, its, scene, sampler, clamping=1e-1):
-        """du/dn at boundary records (wos/wos3d.py:248-286): kernel
+        """du/dn at boundary records (wos/wos3d.py:97-135): kernel
         P = -1 / (sqrt(2) (1 - cos theta)^1.5), cos theta clamped to
         1 - clamping, antithetic azimuth phi + pi.  Returns grad * n."""
         s = as_sampler(sampler)

@@ -22,14 +22,16 @@ class OursCUDA(Solver):
     epsilon2: float = 1e-3
     clamping: float = 1e-1
     control_variates: bool = True
-    # extensions beyond the reference (all default to its behaviour except
-    # source_in_normal_derivative): also return the Dirichlet-value and
-    # source-parameter gradients of the primal walk, and use the source-aware
-    # normal derivative (wos/wos_with_source.py:154-232) when the scene has a
-    # source -- the reference's OursCUDA ignores f there.
+    # extensions beyond the reference, all defaulting to its behaviour: also
+    # return the Dirichlet-value and source-parameter gradients of the primal
+    # walk, and use the source-aware normal derivative
+    # (wos/wos_with_source.py:154-232) when the scene has a source.  The
+    # reference's OursCUDA calls WoSCUDA.normal_derivative, which ignores f
+    # (wos/wos_grad.py:126, :146), so its shape gradient is biased when
+    # f != 0; source_in_normal_derivative=True removes that bias.
     grad_values: bool = False
     grad_source: bool = False
-    source_in_normal_derivative: bool = True
+    source_in_normal_derivative: bool = False
     use_IS_for_greens: bool = False
 
     project_unterminated = False
@@ -54,5 +56,18 @@ class OursCUDA(Solver):
 
 @dataclass
 class Ours(OursCUDA):
-    """The reference's pure-Dr.Jit Ours (wos/wos_grad.py:57-86) uses the same
-    estimator with projected walks; here it runs the same kernel."""
+    """The reference's pure-Dr.Jit Ours (wos/wos_grad.py:57-86): the same
+    boundary-shape estimator on WoS walks, so the primal walk and the two
+    walks on the inscribed ball all stop at this solver's epsilon (there is
+    no epsilon2) and a walk that reaches nsteps is projected to its closest
+    boundary point (wos/wos.py:43) instead of being dropped; the normal
+    derivative is WoS.normal_derivative (wos/wos.py:59-107), which has no
+    source term."""
+    source_in_normal_derivative: bool = False
+
+    project_unterminated = True
+
+    def adjoint_settings(self, scene, want_dV, want_dg, want_dsrc) -> AdjointSettings:
+        a = super().adjoint_settings(scene, want_dV, want_dg, want_dsrc)
+        a.epsilon2 = float(self.epsilon)
+        return a

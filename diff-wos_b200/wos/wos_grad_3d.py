@@ -1,4 +1,4 @@
-"""3D gradient solver (reference: wos/wos_grad_3d.py:378-411)."""
+"""3D gradient solver (reference: wos/wos_grad_3d.py:104-137)."""
 from __future__ import annotations
 
 from dataclasses import dataclass
@@ -11,8 +11,8 @@ from .wos_grad import OursCUDA
 @dataclass
 class Ours3D(OursCUDA):
     """Boundary-shape estimator on triangle meshes: the 3D normal derivative
-    (wos/wos3d.py:248-286) plus the face tangential derivative
-    (wos/wos3d.py:288-307)."""
+    (wos/wos3d.py:97-135) plus the face tangential derivative
+    (wos/wos3d.py:137-156)."""
     epsilon2: float = 1e-3
     clamping: float = 1e-1
 

@@ -93,10 +93,10 @@ typedef struct wos_params {
 } wos_params;
 
 /* Settings of the differential estimator (OursCUDA / Ours3D,
- * wos/wos_grad.py:113-151, wos/wos_grad_3d.py:378-411):
+ * wos/wos_grad.py:113-151, wos/wos_grad_3d.py:104-137):
  *   epsilon2                    shell width of the walks on the inscribed ball;
  *   clamping                    angle clamp of the off-centred Poisson kernel;
- *   control_variates            subtract u at the boundary point (wos/wos.py:227);
+ *   control_variates            subtract u at the boundary point (wos/wos.py:103);
  *   source_in_normal_derivative use the source-aware normal derivative
  *                               (wos/wos_with_source.py:154-232) when the
  *                               scene has a source (2D);
@@ -214,8 +214,8 @@ WOS_API int wos_solve(wos_scene_t scene, const float *P, int n, const wos_params
 /* ---------------------------------------------------------------- gradients */
 
 /* WoS.normal_derivative(its, scene, sampler, clamping, control_variates)
- * (wos/wos.py:184-232; with source wos/wos_with_source.py:154-232; 3D
- * wos/wos3d.py:248-286): one estimate per record, returned as grad * n_out
+ * (wos/wos.py:59-107; with source wos/wos_with_source.py:154-232; 3D
+ * wos/wos3d.py:97-135): one estimate per record, returned as grad * n_out
  * (n x dim).  Records as from wos_walk_records; walk index p->walk_offset. */
 WOS_API int wos_normal_derivative(wos_scene_t scene, const uint8_t *valid, const float *pt, const float *normal,
                           const float *t_or_uv, const int32_t *prim, int n, const wos_params *p,
@@ -228,7 +228,7 @@ WOS_API size_t wos_adjoint_workspace_size(wos_scene_t scene);
  * to vertex positions (dV, nV x dim), Dirichlet values (dg, nV) and source
  * parameters (dsrc, 5): out += sum_i dLdu[i] d mean_i / d theta.  This is
  * CustomSolver.backward with OursCUDA / Ours3D (wos/solver.py:109-114,
- * wos/wos_grad.py:130-151, wos/wos_grad_3d.py:391-411) plus the gathers the
+ * wos/wos_grad.py:130-151, wos/wos_grad_3d.py:117-137) plus the gathers the
  * forward attaches (wos/scene.py:353-357, wos/wos_with_source.py:89-90).
  * Walks are recomputed from their Philox counters (same seed as the forward
  * solve gives common random numbers).  Outputs are float32 device arrays that
@@ -328,7 +328,14 @@ typedef struct wos_detector {
     int32_t slab_axis;
     float slab_center, slab_half_width;
     float size;
+    int32_t flags; /* WOS_DETECTOR_* bits */
 } wos_detector;
+
+/* wos_detector.flags: divide a 3D sample's pmf by |ab x ac| as the
+ * reference's Scene3D.sample_boundary does (wos/scene3d.py:251, :262), which
+ * is twice the triangle's area and doubles the 3D boundary term; without it
+ * the pdf is the correct 1 / (total area).  2D is the same either way. */
+#define WOS_DETECTOR_REFERENCE_AREA_PDF 1
 
 /* Image-space boundary term of the shape derivative (WoSBoundary,
  * wos/wos_boundary.py:11-31): res[0] * res[1] * nwalks boundary points drawn
@@ -338,8 +345,8 @@ typedef struct wos_detector {
  * motion of the sampled point.  Forward mode: dV_dir (nV x dim) and
  * image_tangent (npixels doubles, added to).  Reverse mode: dLdI (npixels)
  * and dV (nV x dim floats, added to).  Either pair may be NULL.  The 3D pdf
- * is 1 / (total area); the reference divides the triangle pmf by |ab x ac|,
- * twice the area, which doubles its 3D term. */
+ * is 1 / (total area) unless det->flags has WOS_DETECTOR_REFERENCE_AREA_PDF
+ * (the reference's doubled term). */
 WOS_API int wos_boundary_term(wos_scene_t scene, const wos_detector *det, int nwalks, uint64_t seed,
                               const float *dV_dir, double *image_tangent, const float *dLdI, float *dV,
                               wos_stream_t stream);

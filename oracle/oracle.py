@@ -53,6 +53,31 @@ class AdjParams(ctypes.Structure):
     ]
 
 
+class Detector(ctypes.Structure):
+    """Must match wos_detector in include/wos_b200.h."""
+    _fields_ = [
+        ("vmin", ctypes.c_float * 2),
+        ("vmax", ctypes.c_float * 2),
+        ("res", ctypes.c_int32 * 2),
+        ("axis_u", ctypes.c_int32),
+        ("axis_v", ctypes.c_int32),
+        ("slab_axis", ctypes.c_int32),
+        ("slab_center", ctypes.c_float),
+        ("slab_half_width", ctypes.c_float),
+        ("size", ctypes.c_float),
+        ("flags", ctypes.c_int32),
+    ]
+
+
+def make_detector(vmin=(-1.0, -1.0), vmax=(1.0, 1.0), res=(8, 8), axis_u=0, axis_v=1, slab_axis=-1, slab_center=0.0,
+                  slab_half_width=0.0, size=None, flags=0) -> Detector:
+    if size is None:
+        size = (vmax[0] - vmin[0]) * (vmax[1] - vmin[1]) * (2 * slab_half_width if slab_axis >= 0 else 1.0)
+    return Detector((ctypes.c_float * 2)(*vmin), (ctypes.c_float * 2)(*vmax), (ctypes.c_int32 * 2)(*res),
+                    int(axis_u), int(axis_v), int(slab_axis), float(slab_center), float(slab_half_width), float(size),
+                    int(flags))
+
+
 def make_params(nwalks=1, nsteps=32, epsilon=1e-3, double_sided=False, prevent_fd_artifacts=False,
                 use_IS_for_greens=False, include_source=False, project_unterminated=False, use_bvh=True,
                 walk_offset=0, seed=0, jitter=(0.0, 0.0, 0.0)) -> Params:
@@ -109,6 +134,7 @@ def lib() -> ctypes.CDLL:
         L.orc_soft_walk.argtypes = [P, P, I, ctypes.POINTER(Params), P, I]
         L.orc_adjoint_counted.argtypes = [P, P, I, ctypes.POINTER(Params), ctypes.POINTER(AdjParams), P, P, P, P, I,
                                           P]
+        L.orc_boundary_term.argtypes = [P, ctypes.POINTER(Detector), I, ctypes.c_uint64, P, P, P, P, I]
         _lib = L
     return _lib
 
@@ -241,6 +267,19 @@ class OracleScene:
                           _p(dg), _p(ds), nthreads)
         return dV, dg, ds
 
+
+    def boundary_term(self, det: Detector, nwalks, seed=0, dV_dir=None, dLdI=None, nthreads=0):
+        """WoSBoundary's image-space boundary term: the derivative image for
+        vertex motion dV_dir and / or the vertex gradient of pixel weights
+        dLdI (both float64)."""
+        npix = int(det.res[0]) * int(det.res[1])
+        tV = _f32(dV_dir) if dV_dir is not None else None
+        w = _f32(dLdI) if dLdI is not None else None
+        img = np.zeros(npix, np.float64) if tV is not None else None
+        dV = np.zeros(self.V.shape, np.float64) if w is not None else None
+        lib().orc_boundary_term(self.h, ctypes.byref(det), int(nwalks), int(seed) & 0xFFFFFFFFFFFFFFFF, _p(tV),
+                                _p(img), _p(w), _p(dV), nthreads)
+        return img, dV
 
     def soft_walk(self, P, params: Params, nthreads=0):
         """Per-walk values of the soft-edge walk (Baseline), points x walks."""

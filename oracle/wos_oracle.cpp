@@ -21,10 +21,13 @@
 //   scene AABB            include/scene.cuh:428-435
 //   point-triangle        include/util.cuh:22-106 (Ericson, Real-Time
 //                         Collision Detection, sec. 5.1.5)
-//   normal derivative     wos/wos.py:184-232 (2D), wos/wos_with_source.py:
-//                         154-232 (2D with source), wos/wos3d.py:248-286 (3D)
-//   tangent derivative    wos/scene.py:451-460, wos/wos3d.py:288-307
-//   boundary-shape term   wos/wos_grad.py:130-151, wos/wos_grad_3d.py:391-411
+//   normal derivative     wos/wos.py:59-107 (2D), wos/wos_with_source.py:
+//                         154-232 (2D with source), wos/wos3d.py:97-135 (3D)
+//   tangent derivative    wos/scene.py:451-460, wos/wos3d.py:137-156
+//   boundary-shape term   wos/wos_grad.py:113-151 (OursCUDA), :57-86 (Ours),
+//                         wos/wos_grad_3d.py:104-137 (Ours3D)
+//   image boundary term   wos/wos_boundary.py:11-31 with sample_boundary,
+//                         wos/scene.py:435-449, wos/scene3d.py:241-262
 //   get_point / AD glue   wos/scene.py:416-433, wos/scene3d.py:225-239,
 //                         wos/solver.py:49-65, 90-125
 //   LBVH                  Karras, "Maximizing parallelism in the construction
@@ -865,14 +868,15 @@ static float inscribed_ball(const Scene &S, const Rec &r, float eps, bool bvh) {
 }
 
 // u at a point on the inscribed ball: boundary value when within eps2,
-// otherwise a full walk (wos/wos.py:219-223, wos/wos3d.py:275-280).
+// otherwise a full walk (wos/wos.py:94-98, wos/wos3d.py:124-129).
 static float ball_u(const Scene &S, const float *q, const Params &prm, float eps2, const Rng &rng,
                     uint32_t pt, uint32_t wk, uint32_t role, bool with_src) {
     const Hit hit = nearest(S, q, prm.use_bvh != 0);
     const float d = sqrtf(hit.d2);
     if (d < eps2) return dirichlet(S, closest_record(S, q, hit.prim));
+    // the ball walks end like the primal walk: projected (the Dr.Jit WoS,
+    // wos/wos.py:43) or invalid (the CUDA walk, include/wos.cuh:144)
     Params p2 = prm;
-    p2.project_unterminated = 0;
     p2.prevent_fd_artifacts = 0;
     const Rec r = walk(S, q, p2, eps2, rng, pt, wk, role, false, nullptr);
     return walk_value(S, r, with_src);
@@ -965,7 +969,7 @@ static void normal_derivative(const Scene &S, const Rec &rec, const Params &prm,
 }
 
 // Tangential gradient of the Dirichlet data (wos/scene.py:451-460,
-// wos/wos3d.py:288-307).
+// wos/wos3d.py:137-156).
 static void tangent_derivative(const Scene &S, const Rec &rec, float *out) {
     if (S.D == 2) {
         const int *I = &S.F[(size_t)rec.prim * 2];
@@ -1204,6 +1208,147 @@ void orc_soft_walk(void *s, const float *P, int n, const Params *prm, float *val
     for (long long t = 0; t < (long long)n * nw; ++t) {
         const int i = (int)(t / nw), w = (int)(t % nw);
         vals[t] = soft_walk(*S, &P[(size_t)i * S->D], *prm, rng, (uint32_t)i, prm->walk_offset + (uint32_t)w);
+    }
+}
+
+// Must match wos_detector in include/wos_b200.h.
+struct Detector {
+    float vmin[2], vmax[2];
+    int32_t res[2];
+    int32_t axis_u, axis_v, slab_axis;
+    float slab_center, slab_half_width;
+    float size;
+    int32_t flags;
+};
+
+// Image-space boundary term of WoSBoundary (wos/wos_boundary.py:11-31):
+// res[0] * res[1] * nwalks boundary samples.  Sample s draws a primitive with
+// probability proportional to its measure (segment length, triangle area;
+// wos/scene.py:275-279, wos/scene3d.py:150-155) by inverse CDF over the
+// running sums, reusing the uniform inside the primitive's interval as the
+// segment parameter (Mitsuba's sample_reuse_pmf, wos/scene.py:435-449); a
+// triangle point is (sqrt r1 (1 - r2), sqrt r1 r2) in barycentrics
+// (wos/scene3d.py:253-257).  n is the detached normal (-ab.y, ab.x) / |ab| or
+// -(ab x ac) / |ab x ac|, val the interpolated Dirichlet value.  The term
+// -val (x . n - detach(x . n)) / pdf has derivative -val (n . dx) / pdf for a
+// motion dx of the sample, the lerp / barycentric mix of its vertices'
+// motion; it goes to the sample's pixel (Detector.index, wos/scene.py:18-24,
+// wos/scene3d.py:35-43), divided by the detector size and nwalks
+// (wos/wos_boundary.py:13-21).  pdf = 1 / total measure, or in 3D with
+// flags & 1 the reference's pmf / |ab x ac| = 1 / (2 total area)
+// (wos/scene3d.py:262).  Random numbers: Philox(seed; s mod 2^32, s / 2^32,
+// 0, role 5).  Forward mode adds the derivative image for vertex motion tV to
+// img; reverse mode adds the vertex gradient of pixel weights dLdI to dV.
+static void boundary_sample(const Scene &S, const Detector &det, const std::vector<double> &cdf, double pdf_scale,
+                            int nwalks, const Rng &rng, long long s, const float *tV, double *img,
+                            const float *dLdI, double *dV) {
+    const int D = S.D;
+    const int nF = S.nF;
+    const double total = cdf[nF - 1];
+    const U4 r = rng.draw((uint32_t)s, (uint32_t)(s >> 32), 0, 5);
+    const double target = (double)wosm::u01(r.x) * total;
+    const int f = (int)(std::upper_bound(cdf.begin(), cdf.end() - 1, target) - cdf.begin());
+    const double base = f > 0 ? cdf[f - 1] : 0.0;
+    const double wdt = cdf[f] - base;
+    float t = wdt > 0.0 ? (float)((target - base) / wdt) : 0.0f;
+    t = fminf(fmaxf(t, 0.0f), 0x1.fffffep-1f);
+    int vid[3] = {0, 0, 0};
+    float wts[3] = {0.0f, 0.0f, 0.0f}, x[3] = {0.0f, 0.0f, 0.0f}, n[3] = {0.0f, 0.0f, 0.0f};
+    float val;
+    if (D == 2) {
+        vid[0] = S.F[2 * f];
+        vid[1] = S.F[2 * f + 1];
+        const float ax = S.V[2 * vid[0]], ay = S.V[2 * vid[0] + 1];
+        const float abx = S.V[2 * vid[1]] - ax, aby = S.V[2 * vid[1] + 1] - ay;
+        x[0] = fmaf(t, abx, ax);
+        x[1] = fmaf(t, aby, ay);
+        wts[0] = 1.0f - t;
+        wts[1] = t;
+        val = fmaf(t, S.g[vid[1]] - S.g[vid[0]], S.g[vid[0]]);
+        const float l = sqrtf(fmaf(abx, abx, aby * aby));
+        n[0] = -aby / l;
+        n[1] = abx / l;
+    } else {
+        for (int k = 0; k < 3; ++k) vid[k] = S.F[3 * f + k];
+        const float su = sqrtf(wosm::u01(r.y)), r2 = wosm::u01(r.z);
+        const float u = su * (1.0f - r2), v = su * r2;
+        wts[0] = 1.0f - u - v;
+        wts[1] = u;
+        wts[2] = v;
+        float ab[3], ac[3];
+        for (int k = 0; k < 3; ++k) {
+            const float a = S.V[3 * vid[0] + k];
+            ab[k] = S.V[3 * vid[1] + k] - a;
+            ac[k] = S.V[3 * vid[2] + k] - a;
+            x[k] = fmaf(u, ab[k], fmaf(v, ac[k], a));
+        }
+        val = fmaf(wts[0], S.g[vid[0]], fmaf(u, S.g[vid[1]], v * S.g[vid[2]]));
+        float c[3];
+        cross3(ab, ac, c);
+        const float l = sqrtf(dot3(c, c));
+        for (int k = 0; k < 3; ++k) n[k] = -c[k] / l;
+    }
+    const int iu = (int)fmaf((x[det.axis_u] - det.vmin[0]) / (det.vmax[0] - det.vmin[0]), (float)det.res[0], 0.5f);
+    const int iv = (int)fmaf((x[det.axis_v] - det.vmin[1]) / (det.vmax[1] - det.vmin[1]), (float)det.res[1], 0.5f);
+    bool ok = iu >= 0 && iu < det.res[0] && iv >= 0 && iv < det.res[1];
+    if (det.slab_axis >= 0) ok = ok && fabsf(x[det.slab_axis] - det.slab_center) < det.slab_half_width;
+    const long long npix = (long long)det.res[0] * det.res[1];
+    const long long idx = (long long)iu + (long long)(det.res[1] - iv) * det.res[0];
+    if (!ok || idx < 0 || idx >= npix) return;
+    const double w = -(double)val * total * pdf_scale / ((double)det.size * nwalks);
+    if (tV != nullptr) {
+        double nd = 0.0;
+        for (int j = 0; j < D; ++j)
+            for (int k = 0; k < D; ++k) nd += (double)n[k] * wts[j] * tV[(size_t)vid[j] * D + k];
+        img[idx] += w * nd;
+    }
+    if (dLdI != nullptr) {
+        const double cw = (double)dLdI[idx] * w;
+        for (int j = 0; j < D; ++j)
+            for (int k = 0; k < D; ++k) dV[(size_t)vid[j] * D + k] += cw * n[k] * wts[j];
+    }
+}
+
+void orc_boundary_term(void *s, const Detector *det, int nwalks, uint64_t seed, const float *tV, double *img,
+                       const float *dLdI, double *dV, int nthreads) {
+    Scene *S = (Scene *)s;
+    const int D = S->D;
+    const int nF = S->nF;
+    std::vector<double> cdf(nF);
+    double run = 0.0;
+    for (int f = 0; f < nF; ++f) {
+        double m;
+        if (D == 2) {
+            const float *a = &S->V[2 * S->F[2 * f]], *b = &S->V[2 * S->F[2 * f + 1]];
+            const double dx = (double)b[0] - a[0], dy = (double)b[1] - a[1];
+            m = sqrt(dx * dx + dy * dy);
+        } else {
+            const float *a = &S->V[3 * S->F[3 * f]], *b = &S->V[3 * S->F[3 * f + 1]], *c = &S->V[3 * S->F[3 * f + 2]];
+            const double u[3] = {(double)b[0] - a[0], (double)b[1] - a[1], (double)b[2] - a[2]};
+            const double v[3] = {(double)c[0] - a[0], (double)c[1] - a[1], (double)c[2] - a[2]};
+            const double cx = u[1] * v[2] - u[2] * v[1], cy = u[2] * v[0] - u[0] * v[2], cz = u[0] * v[1] - u[1] * v[0];
+            m = 0.5 * sqrt(cx * cx + cy * cy + cz * cz);
+        }
+        run += m;
+        cdf[f] = run;
+    }
+    const double pdf_scale = (D == 3 && (det->flags & 1)) ? 2.0 : 1.0;
+    const long long npix = (long long)det->res[0] * det->res[1];
+    const long long ns = npix * nwalks;
+    const Rng rng = make_rng(seed);
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    const size_t nvd = (size_t)S->nV * D;
+#pragma omp parallel
+    {
+        std::vector<double> im(tV ? npix : 0, 0.0), dv(dLdI ? nvd : 0, 0.0);
+#pragma omp for schedule(static)
+        for (long long i = 0; i < ns; ++i)
+            boundary_sample(*S, *det, cdf, pdf_scale, nwalks, rng, i, tV, im.data(), dLdI, dv.data());
+#pragma omp critical
+        {
+            for (size_t k = 0; k < im.size(); ++k) img[k] += im[k];
+            for (size_t k = 0; k < dv.size(); ++k) dV[k] += dv[k];
+        }
     }
 }
 

@@ -50,6 +50,8 @@ def test_oracle_params_match_library_params():
     from wos import _lib
     assert [f[0] for f in O.Params._fields_] == [f[0] for f in _lib.WosParams._fields_]
     assert [f[0] for f in O.AdjParams._fields_] == [f[0] for f in _lib.WosAdjointParams._fields_]
+    assert [f[0] for f in O.Detector._fields_] == [f[0] for f in _lib.WosDetector._fields_]
+    assert ctypes.sizeof(O.Detector) == ctypes.sizeof(_lib.WosDetector) == 52
 
 
 def test_argument_validation_without_gpu():

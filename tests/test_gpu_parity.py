@@ -304,7 +304,7 @@ def test_autograd_custom_solver_matches_native(cuda, oracle):
     scene = wos.Polyline(Vt, F, gt, source_type=2, source_params=st)
     fwd = wos.WoSWithSourceCUDA(nwalks=16, nsteps=64, use_IS_for_greens=True)
     bwd = wos.OursCUDA(nwalks=16, nsteps=64, epsilon=1e-3, epsilon2=1e-3, grad_values=True, grad_source=True,
-                       use_IS_for_greens=True)
+                       use_IS_for_greens=True, source_in_normal_derivative=True)
     u = wos.CustomSolver(fwd, bwd).walk(P, scene, seed=9)
     (u * u).mean().backward()
     ns = scene._native

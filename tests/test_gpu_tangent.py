@@ -119,3 +119,46 @@ def test_forward_ad_derivative_image(cuda):
     rhs = float((Vr.grad.double() * dirV.double()).sum())
     assert abs(lhs - rhs) <= 1e-4 * max(abs(rhs), 1e-6), (lhs, rhs)
     assert wos.device_status() == 0
+
+
+def _odet(oracle, c):
+    """The same wos_detector for the oracle."""
+    return oracle.make_detector(tuple(c.vmin), tuple(c.vmax), tuple(c.res), c.axis_u, c.axis_v, c.slab_axis,
+                                c.slab_center, c.slab_half_width, c.size, c.flags)
+
+
+@pytest.mark.parametrize("kind,reference_pdf", [("star", False), ("star", True), ("sphere", False),
+                                                ("sphere", True)])
+def test_boundary_term_matches_oracle(cuda, oracle, kind, reference_pdf):
+    """wos_boundary_term (k_boundary) against the oracle's restatement of
+    WoSBoundary (wos/wos_boundary.py:11-31): same Philox samples, so the same
+    primitives, pixels and contributions; the images and vertex gradients
+    differ only by FP64 summation order.  With the reference's 3D pdf the 3D
+    term is twice the default one; 2D is unchanged."""
+    import torch
+    import wos
+    from wos.native import NativeScene
+    rng = np.random.default_rng(12)
+    if kind == "star":
+        V, F, g = star_scene(512)
+        det = wos.Detector(vmin=(-1.0, -1.0), vmax=(1.0, 1.0), res=(24, 20))
+    else:
+        V, F, g = sphere_scene(2)
+        det = wos.Detector3D(vmin=(-1.2, -1.2), vmax=(1.2, 1.2), res=(24, 20), z=0.05)
+    ns = NativeScene(V, F, g)
+    os_ = oracle.OracleScene(V, F, g)
+    wb = wos.WoSBoundary(nwalks=64, reference_area_pdf=reference_pdf)
+    c = det.c(wb.flags())
+    dV = rng.normal(size=V.shape).astype(np.float32)
+    dLdI = rng.normal(size=det.res[0] * det.res[1]).astype(np.float32)
+    img, gV = ns.boundary_term(c, 64, 9, dV_dir=torch.tensor(dV, device="cuda"),
+                               dLdI=torch.tensor(dLdI, device="cuda"))
+    oimg, ogV = os_.boundary_term(_odet(oracle, c), 64, 9, dV_dir=dV, dLdI=dLdI)
+    assert np.count_nonzero(oimg) > 20
+    np.testing.assert_allclose(_np(img), oimg, rtol=1e-9, atol=1e-12 * np.abs(oimg).max())
+    np.testing.assert_allclose(_np(gV), ogV, rtol=1e-5, atol=1e-6 * np.abs(ogV).max())
+    base, _ = ns.boundary_term(det.c(0), 64, 9, dV_dir=torch.tensor(dV, device="cuda"))
+    factor = 2.0 if (reference_pdf and kind == "sphere") else 1.0
+    # atomics add in a different order on every launch
+    np.testing.assert_allclose(_np(img), factor * _np(base), rtol=1e-12, atol=1e-14 * np.abs(oimg).max())
+    assert wos.device_status() == 0

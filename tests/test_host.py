@@ -106,6 +106,15 @@ def test_solver_semantics_match_reference_classes():
     assert (a.want_dV, a.want_dg, a.want_dsrc) == (True, False, False)
     a = wos.OursCUDA(grad_values=True, grad_source=True, epsilon2=5e-4).adjoint_settings(s, True, True, True)
     assert (a.want_dV, a.want_dg, a.want_dsrc, a.epsilon2) == (True, True, True, 5e-4)
+    # the reference's OursCUDA uses the source-blind normal derivative (wos/wos_grad.py:146)
+    assert wos.OursCUDA().adjoint_settings(s, True, True, True).source_in_normal_derivative is False
+    assert wos.OursCUDA(source_in_normal_derivative=True).adjoint_settings(s, True, False, False) \
+        .source_in_normal_derivative is True
+    # the reference's Ours: WoS walks (projected at nsteps) at epsilon for the primal and the ball walks
+    o = wos.Ours(epsilon=2e-3, epsilon2=7e-4)
+    assert o.adjoint_settings(s, True, False, False).epsilon2 == 2e-3
+    assert o.walk_settings(s).project_unterminated is True
+    assert wos.OursCUDA().walk_settings(s).project_unterminated is False
 
 
 def test_sampler_advances():
