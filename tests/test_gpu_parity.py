@@ -354,3 +354,29 @@ def test_walk_detector_jittered_pixels(cuda, oracle):
     odV, _, _ = os_.adjoint(P, _oparams(oracle, s), oa, dLdu)
     np.testing.assert_allclose(_np(Vt.grad), odV, rtol=GRAD_RTOL, atol=GRAD_RTOL * np.abs(odV).max())
     assert wos.device_status() == 0
+
+
+@pytest.mark.parametrize("kind", ["circle", "sphere"])
+def test_projected_walk_adjoint_matches_oracle(cuda, oracle, kind):
+    """Walks that reach nsteps are projected to their closest boundary point
+    (the Dr.Jit WoS, wos/wos.py:43) in the primal walk and in the walks on the
+    inscribed ball, as the reference's Ours does (wos/wos_grad.py:57-86);
+    nsteps 6 makes many walks end that way."""
+    from wos.native import AdjointSettings
+    V, F, g = {"circle": lambda: circle_scene(256), "sphere": lambda: sphere_scene(2)}[kind]()
+    ns, os_ = _scenes(oracle, V, F, g)
+    P = _pts2(200, 13, -0.6, 0.6) if V.shape[1] == 2 else _pts3(150, 13, -0.5, 0.5)
+    rng = np.random.default_rng(13)
+    dLdu = rng.normal(size=len(P)).astype(np.float32)
+    s = _settings(nwalks=8, nsteps=6, seed=17, project_unterminated=True)
+    a = AdjointSettings(epsilon2=1e-3, clamping=0.1, want_dV=True, want_dg=True)
+    dV, dg, _ = ns.adjoint(P, s, a, dLdu)
+    odV, odg, _ = os_.adjoint(P, _oparams(oracle, s), oracle.make_adj(1e-3, 0.1, True, False, 1e-3, True, True, False),
+                              dLdu)
+    np.testing.assert_allclose(_np(dV), odV, rtol=GRAD_RTOL, atol=GRAD_RTOL * np.abs(odV).max())
+    np.testing.assert_allclose(_np(dg), odg, rtol=GRAD_RTOL, atol=GRAD_RTOL * np.abs(odg).max())
+    # records at a single walk: the normal derivative with projected ball walks
+    s1 = _settings(nwalks=1, nsteps=6, seed=18, project_unterminated=True)
+    orec = os_.walk_records(P, _oparams(oracle, s1))
+    nd = _np(ns.normal_derivative(orec, s1, a))
+    assert np.array_equal(nd, os_.normal_derivative(orec, _oparams(oracle, s1), oracle.make_adj(1e-3, 0.1)))
