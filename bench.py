@@ -18,12 +18,15 @@ e2e     the same metric through the public Python API (wos.CustomSolver with
         WoSWithSourceCUDA forward and OursCUDA backward, torch autograd) with
         host buffers: H2D of points and scene, scene build, forward, backward,
         D2H of loss and gradients inside the timed region.
-roofline  the adjoint kernel (the dominant one): algorithmic bytes per launch
-        (32 B per LBVH node visit + 16 B per segment test, counted on the
-        device for this exact launch) / its CUDA-event time, against the
-        measured HBM copy bandwidth.  `issue` gives FP32 algorithmic ops
-        (12 per node visit, 20 per segment test, 10 per query) against
-        148 SMs x 128 lanes x 2 x SM clock.
+roofline  the adjoint kernel (the dominant one), which is bound by
+        instruction issue: warp instructions per nearest query (from the ncu
+        capture in profiles/) x the launch's queries (device counters) / its
+        CUDA-event time, against 148 SMs x 4 schedulers x the SM clock.
+        Beside it: `ref_lbvh_bytes`, the reference LBVH traversal's box and
+        primitive bytes for the same samples over the HBM copy peak (served
+        from L1/L2), and `fp32_algorithmic`, the reference algorithm's FP32
+        ops (12 per node visit, 20 per segment test, 10 per query) over
+        148 SMs x 128 lanes x 2 x SM clock; `traffic` is DRAM bytes.
 --impl reference  the CPU restatement of the reference algorithm (the
         reference itself cannot run: it needs Dr.Jit/Mitsuba and the lbvh
         submodule), all host threads, bounded samples of the same workload.
@@ -235,7 +238,11 @@ def reference_arm(args, world, rank):
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_config(len(P), per_step_points=n),
+        "config": workload_config(len(P)),
+        "sample": {"points_per_step": n, "of_points": len(P), "walks_per_point": NWALKS,
+                   "note": "each step runs the forward walks and adjoint samples of an evenly spaced subset of the "
+                           "workload's points (a bounded CPU sample); walks/s is per walk, so it compares with "
+                           "the full-workload GPU figure"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{n} of {len(P)} points x {NWALKS} walks (forward + adjoint), oracle C++ "
                                    f"restatement, {threads} threads, {cpu_info()}"},
@@ -247,14 +254,12 @@ def reference_arm(args, world, rank):
     return 0
 
 
-def workload_config(npts, per_step_points=None):
+def workload_config(npts):
     c = {"workload": f"2d_differentiable_solve_star4096_grid{GRID}_walks{NWALKS}",
          "scene": "star r=0.6+0.25cos(5t), 4096 segments", "points": npts, "walks_per_point": NWALKS,
          "nsteps": NSTEPS, "epsilon": EPS, "epsilon2": EPS2, "source": "f=1, G-CDF importance sampling",
          "loss": "mean(u^2); adjoint wrt g, f, vertex xy", "nearest": "LBVH",
          "l2": "inputs < L2; 256 MiB buffer written between timed steps (L2 flush)"}
-    if per_step_points is not None:
-        c["points_per_step"] = per_step_points
     return c
 
 
@@ -722,14 +727,15 @@ def fd_check(make_scene, V, P_d, settings, adjoint, seeds, nvert=32, hs=(1e-3, 5
                "checks": checks}
 
 
-def fd_line(workload, npts, seeds, t, res, note):
+def fd_line(workload, npts, seeds, t, res, note, hs, eps):
+    h0 = f"h{hs[0]:g}"
     return {
-        "metric": "vertex_gradient_fd_check", "value": res["checks"]["h0.001"]["within_2se"],
-        "unit": "fraction of vertices within 2 SE (h = 1e-3)", "n_gpus": 1, "steps": seeds, "warmup": 0,
+        "metric": "vertex_gradient_fd_check", "value": res["checks"][h0]["within_2se"],
+        "unit": f"fraction of vertices within 2 SE (h = {hs[0]:g})", "n_gpus": 1, "steps": seeds, "warmup": 0,
         "ms_per_step": t / seeds * 1e3, "higher_is_better": True, "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": workload, "points": npts, "points_note": note, "h": [1e-3, 5e-4], "seeds": seeds,
-                   "fd": "central, common random numbers"},
+        "config": {"workload": workload, "points": npts, "points_note": note, "h": list(hs), "epsilon": eps,
+                   "seeds": seeds, "fd": "central, common random numbers"},
         **res,
     }
 
@@ -754,9 +760,9 @@ def fd_main(args):
     V, F, g, P = make_workload()
     P = np.ascontiguousarray(P[shapes.inside_star(P, STAR["r0"], STAR["amp"], STAR["lobes"], margin=0.01)])
     t, res = fd_check(lambda: NativeScene(V, F, g, 2, SOURCE), V, torch.as_tensor(P, device=dev), walk_settings,
-                      adjoint_settings(), args.seeds)
+                      adjoint_settings(), args.seeds, hs=args.fd_h)
     print(json.dumps(fd_line(workload_config(len(P))["workload"], len(P), args.seeds, t, res,
-                             "grid points at least 0.01 inside the boundary")), flush=True)
+                             "grid points at least 0.01 inside the boundary", args.fd_h, EPS)), flush=True)
     return 0
 
 
@@ -774,14 +780,15 @@ def c3fd_main(args):
     g = shapes.harmonic_c3(V).astype(np.float32)
     P = shapes.sample_interior_3d(20000, shapes.displaced_radius_fn(0.15, 0), seed=2, margin=0.01)
     P = np.ascontiguousarray(P[:20000]).astype(np.float32)
-    adj = AdjointSettings(epsilon2=1e-3, clamping=0.1, want_dV=True, want_dg=True, want_dsrc=False)
+    adj = AdjointSettings(epsilon2=EPS2, clamping=0.1, want_dV=True, want_dg=True, want_dsrc=False)
 
     def ws(seed):
-        return WalkSettings(nwalks=128, nsteps=64, epsilon=1e-3, seed=seed)
+        return WalkSettings(nwalks=128, nsteps=64, epsilon=EPS, seed=seed)
 
-    t, res = fd_check(lambda: NativeScene(V, F, g), V, torch.as_tensor(P, device=dev), ws, adj, args.seeds)
+    t, res = fd_check(lambda: NativeScene(V, F, g), V, torch.as_tensor(P, device=dev), ws, adj, args.seeds,
+                      hs=args.fd_h)
     print(json.dumps(fd_line("3d_forward_adjoint_icosphere81920_pts20000_walks128", len(P), args.seeds, t, res,
-                             "seeded interior points at least 0.01 inside (radially)")), flush=True)
+                             "seeded interior points at least 0.01 inside (radially)", args.fd_h, EPS)), flush=True)
     return 0
 
 
@@ -861,11 +868,18 @@ def main():
                          "c3: the 3D forward + adjoint solve; c4: the 2D inverse problem; "
                          "batched: many scenes in one launch")
     ap.add_argument("--seeds", type=int, default=16, help="seeds of the c2fd gradient check")
+    ap.add_argument("--fd-h", default="1e-3,5e-4", help="c2fd / c3fd: comma-separated finite-difference steps")
+    ap.add_argument("--fd-eps", type=float, default=None,
+                    help="c2fd / c3fd: termination shell epsilon of the walks and the ball walks (default 1e-3)")
     ap.add_argument("--iters", type=int, default=500, help="Adam iterations of the c4 workload")
     ap.add_argument("--points", type=int, default=1_000_000, help="query points of the c3 workload")
     ap.add_argument("--scale", type=float, default=0.1, help="query-count scale of the batched workload")
     args = ap.parse_args()
     set_size(args.grid, args.walks if args.walks is not None else NWALKS)
+    args.fd_h = tuple(float(x) for x in args.fd_h.split(","))
+    if args.fd_eps is not None:
+        global EPS, EPS2
+        EPS = EPS2 = float(args.fd_eps)
     if args.workload == "batched" and args.impl == "ours":
         return batched_main(args)
     if args.workload == "c1" and args.impl == "ours":
@@ -1018,11 +1032,14 @@ def main():
     sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6
     traffic = None
+    ipq = None
+    tj = {}
     tp = ROOT / "profiles" / "roofline_traffic.json"
     if tp.exists():
         tj = json.load(open(tp))
         if tj.get("kernel") == "k_adjoint" and tj.get("workload") == workload_config(n)["workload"]:
             traffic = tj.get("traffic_bytes_per_launch")
+            ipq = tj.get("warp_instructions_per_query")
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -1043,6 +1060,23 @@ def main():
         line["clocks"] = clk
     if e2e is not None:
         line["e2e"] = e2e
+    # issue roofline of the adjoint kernel: warp instructions per nearest
+    # query (ncu capture of the same kernel) x this launch's queries (device
+    # counters) / its CUDA-event time, against one warp instruction per cycle
+    # on each of the 4 schedulers of 148 SMs at the median SM clock
+    issue_peak = 148 * 4 * sm_mhz * 1e6
+    if ipq is not None:
+        inst = float(ipq) * adj_work["queries"]
+        line["roofline"] = {
+            "bound": "issue", "achieved": inst / adj_avg / 1e9, "peak": issue_peak / 1e9, "unit": "Ginst/s",
+            "frac": inst / adj_avg / issue_peak, "traffic": traffic, "kernel": "k_adjoint",
+            "peak_kind": f"148 SMs x 4 warp schedulers x {sm_mhz:.0f} MHz (median SM clock of the timed region)",
+            "per_unit": {"unit": "nearest query (one warp-cooperative wide-tree search)",
+                         "warp_instructions_per_query": ipq, "queries_per_launch": adj_work["queries"],
+                         "source": tj.get("instructions_measured_on")},
+            "note": "the scene and trees (~0.2 MB) stay in L1/L2 and DRAM traffic is the per-walk records "
+                    "(`traffic`, bytes per launch); the kernel is bound by instruction issue",
+        }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         S, prm, adjp, run, m, threads = cpu_baseline(V, F, g, P)
         ts = [run(m) for _ in range(2)]
@@ -1056,18 +1090,19 @@ def main():
         samples = n * NWALKS
         adj_bytes, adj_ops = algorithmic({k: v * samples for k, v in ref["adjoint"].items()})
         achieved = adj_bytes / adj_avg / 1e9
-        line["roofline"] = {
-            "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-            "traffic": traffic, "kernel": "k_adjoint", "peak_kind": peak_kind,
+        line.setdefault("roofline", {"bound": "issue", "achieved": None, "peak": issue_peak / 1e9,
+                                     "unit": "Ginst/s", "frac": None, "traffic": traffic, "kernel": "k_adjoint"})
+        line["roofline"]["ref_lbvh_bytes"] = {
+            "achieved_gbs": achieved, "peak_gbs": hbm, "peak_kind": peak_kind, "frac": achieved / hbm,
             "algorithmic_bytes_per_launch": adj_bytes,
             "per_unit": {"unit": "adjoint sample (one walk's boundary-shape + normal-derivative estimate)",
                          "reference_lbvh_work": ref["adjoint"], "forward_walk_work": ref["forward"],
                          "sample": ref["sample"]},
-            "issue": {"achieved_tflops": adj_ops / adj_avg / 1e12, "peak_tflops": fp32_peak / 1e12,
-                      "frac": adj_ops / adj_avg / fp32_peak},
-            "note": "the scene and tree (~0.2 MB) stay in L1/L2; algorithmic bytes are the reference "
-                    "traversal's box and primitive reads, served from cache, not HBM traffic",
+            "note": "the reference binary LBVH traversal's box and primitive reads for the same samples, over "
+                    "the HBM copy peak; they are served from L1/L2, not HBM",
         }
+        line["roofline"]["fp32_algorithmic"] = {"achieved_tflops": adj_ops / adj_avg / 1e12,
+                                                "peak_tflops": fp32_peak / 1e12, "frac": adj_ops / adj_avg / fp32_peak}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

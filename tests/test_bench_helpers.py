@@ -41,9 +41,12 @@ def test_walk_steps_histogram(bench):
 def test_fd_line_reports_the_configured_step(bench):
     res = {"vertices": [1, 2], "adjoint_mean": [0.0, 1.0],
            "checks": {"h0.001": {"within_2se": 0.5}, "h0.0005": {"within_2se": 1.0}}}
-    line = bench.fd_line("w", 10, 4, 2.0, res, "note")
+    line = bench.fd_line("w", 10, 4, 2.0, res, "note", (1e-3, 5e-4), 1e-3)
     assert line["value"] == 0.5 and line["ms_per_step"] == 500.0
     assert line["checks"]["h0.0005"]["within_2se"] == 1.0
+    assert line["config"]["h"] == [1e-3, 5e-4] and line["config"]["epsilon"] == 1e-3
+    # the headline value is the first step asked for
+    assert bench.fd_line("w", 10, 4, 2.0, res, "note", (5e-4, 1e-3), 1e-2)["value"] == 1.0
 
 
 def test_c3_cpu_baseline_small(bench, oracle):
