@@ -610,6 +610,35 @@ int wos_soft_walk(wos_scene_t scene, const float *P, int n, const wos_params *p,
     return 0;
 }
 
+int wos_soft_walk_adjoint(wos_scene_t scene, const float *P, int n, const wos_params *p, const float *dLdu, float *dV,
+                          float *dg, wos_stream_t stream) {
+    if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (int rc = check_params(p)) return rc;
+    if (p->nsteps < 1) return fail(WOS_ERR_INVALID_ARGUMENT, "the soft-edge walk needs nsteps >= 1");
+    if (!(p->epsilon > 0.0f)) return fail(WOS_ERR_INVALID_ARGUMENT, "the soft-edge walk needs epsilon > 0");
+    if (n < 0) return fail(WOS_ERR_INVALID_ARGUMENT, "n must be >= 0");
+    if (n == 0 || (dV == nullptr && dg == nullptr)) return 0;
+    WOS_CHECK_DEV(P, "P");
+    WOS_CHECK_DEV(dLdu, "dLdu");
+    WOS_CHECK_DEV_OPT(dV, "dV");
+    WOS_CHECK_DEV_OPT(dg, "dg");
+    const SceneImpl &S = scene->impl;
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long nvd = (long long)S.nV * S.dim;
+    double *acc = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&acc, sizeof(double) * (size_t)(nvd + S.nV), st);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMallocAsync(soft adjoint accumulators)");
+    e = cudaMemsetAsync(acc, 0, sizeof(double) * (size_t)(nvd + S.nV), st);
+    int rc = e == cudaSuccess ? 0 : fail_cuda(e, "cudaMemsetAsync(soft adjoint accumulators)");
+    if (rc == 0)
+        rc = launch_soft_adjoint(S, P, (long long)n * p->nwalks, *p, dLdu, acc, dg != nullptr ? acc + nvd : nullptr,
+                                 st);
+    if (rc == 0 && dV != nullptr) rc = launch_add_f64(acc, dV, nvd, st);
+    if (rc == 0 && dg != nullptr) rc = launch_add_f64(acc + nvd, dg, S.nV, st);
+    cudaFreeAsync(acc, st);
+    return rc;
+}
+
 int wos_boundary_term(wos_scene_t scene, const wos_detector *det, int nwalks, uint64_t seed, const float *dV_dir,
                       double *image_tangent, const float *dLdI, float *dV, wos_stream_t stream) {
     if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");

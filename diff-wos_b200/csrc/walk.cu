@@ -1467,6 +1467,226 @@ __global__ void __launch_bounds__(256) k_walk_soft(SceneView S, WalkCfg c, const
     if (c.count) flush_work<BVH>(work);
 }
 
+// ------------------------------------------------------------------ soft-edge walk, reverse mode
+// Transposed step of the soft walk's tangent recurrence (k_walk_soft): given
+// the adjoint gbar of the step's boundary-value tangent gd, add the adjoints
+// of the position tangent (pbar) and of the vertex motion (dV, FP64 atomics)
+// that enter gd through the motion of the closest point's barycentrics
+// (soft_tangents: proj_dot along an edge, the 2 x 2 normal equations on a
+// face).
+template <int D>
+__device__ void soft_bary_adjoint(const SceneView &S, const float *x, const Rec &r, int prim, const int *vid,
+                                  float gbar, float *pbar, double *dV) {
+    float V[3][3], gv[3];
+    for (int j = 0; j < D; ++j) {
+        gv[j] = __ldg(&S.g[vid[j]]);
+        for (int k = 0; k < 3; ++k) V[j][k] = k < D ? __ldg(&S.V[(size_t)vid[j] * D + k]) : 0.0f;
+    }
+    // an edge (i0 -> i1) at parameter t: bd[i1] = td, bd[i0] = -td
+    auto edge = [&](int i0, int i1, float t) {
+        const float tbar = gbar * (gv[i1] - gv[i0]);
+        float e[3], xa[3], ee = 0.0f;
+        for (int k = 0; k < D; ++k) {
+            e[k] = V[i1][k] - V[i0][k];
+            xa[k] = x[k] - V[i0][k];
+            ee += e[k] * e[k];
+        }
+        if (!(ee > 0.0f) || tbar == 0.0f) return;
+        for (int k = 0; k < D; ++k) {
+            const float ce = tbar * e[k] / ee;                        // d td / d xd, -d td / d ad
+            const float ced = tbar * (xa[k] - 2.0f * t * e[k]) / ee;  // d td / d ed
+            pbar[k] += ce;
+            atomicAdd(&dV[(size_t)vid[i0] * D + k], (double)(-ce - ced));
+            atomicAdd(&dV[(size_t)vid[i1] * D + k], (double)ced);
+        }
+    };
+    if (D == 2) {
+        if (r.t0 > 0.0f && r.t0 < 1.0f) edge(0, 1, r.t0);
+        return;
+    }
+    const float4 t0 = __ldg(&S.tri[3 * prim]), t1 = __ldg(&S.tri[3 * prim + 1]), t2 = __ldg(&S.tri[3 * prim + 2]);
+    const int reg = tri_region(t0, t1, t2, x);
+    if (reg == 3) {
+        edge(0, 1, r.t0);
+    } else if (reg == 4) {
+        edge(0, 2, r.t1);
+    } else if (reg == 5) {
+        edge(1, 2, r.t1);
+    } else if (reg == 6) {
+        float ab[3], ac[3], xa[3], G00 = 0, G01 = 0, G11 = 0;
+        for (int k = 0; k < 3; ++k) {
+            ab[k] = V[1][k] - V[0][k];
+            ac[k] = V[2][k] - V[0][k];
+            xa[k] = x[k] - V[0][k];
+            G00 += ab[k] * ab[k];
+            G01 += ab[k] * ac[k];
+            G11 += ac[k] * ac[k];
+        }
+        const float det = G00 * G11 - G01 * G01;
+        if (det == 0.0f) return;
+        // gd = vd (g1 - g0) + wd (g2 - g0), [vd wd] = G^-1 [q0 q1]
+        const float vbar = gbar * (gv[1] - gv[0]), wbar = gbar * (gv[2] - gv[0]);
+        const float q0 = (G11 * vbar - G01 * wbar) / det, q1 = (G00 * wbar - G01 * vbar) / det;
+        const float v = r.t0, w = r.t1;
+        for (int k = 0; k < 3; ++k) {
+            const float cx = q0 * ab[k] + q1 * ac[k];  // via xd - ad
+            const float cab = q0 * (xa[k] - 2.0f * v * ab[k] - w * ac[k]) - q1 * v * ac[k];
+            const float cac = -q0 * w * ab[k] + q1 * (xa[k] - v * ab[k] - 2.0f * w * ac[k]);
+            pbar[k] += cx;
+            atomicAdd(&dV[(size_t)vid[0] * 3 + k], (double)(-cx - cab - cac));
+            atomicAdd(&dV[(size_t)vid[1] * 3 + k], (double)cab);
+            atomicAdd(&dV[(size_t)vid[2] * 3 + k], (double)cac);
+        }
+    }
+}
+
+// Direction of step i of the soft walk (pt, wk), as k_walk_soft draws it.
+template <int D>
+__device__ __forceinline__ void soft_dir(const WalkCfg &c, uint32_t pt, uint32_t wk, int i, float *dir) {
+    const uint4 rr = philox(c.rng, pt, wk, (uint32_t)i, ROLE_PRIMAL);
+    dir[2] = 0.0f;
+    if (D == 2) {
+        float sn, cs;
+        wosm::sincos_2pi(wosm::u01(rr.x), &sn, &cs);
+        dir[0] = cs;
+        dir[1] = sn;
+    } else {
+        const float z = fmaf(-2.0f, wosm::u01(rr.x), 1.0f);
+        const float rad = sqrtf(fmaxf(0.0f, fmaf(-z, z, 1.0f)));
+        float sn, cs;
+        wosm::sincos_2pi(wosm::u01(rr.y), &sn, &cs);
+        dir[0] = rad * cs;
+        dir[1] = rad * sn;
+        dir[2] = z;
+    }
+}
+
+// Reverse mode of the soft-edge walk: for walks [w0, w0 + nchunk) of the
+// flattened (point, walk) space, add dL/du[point] / nwalks times the walk's
+// derivative with respect to vertex positions (dV) and values (dg).  One
+// thread per walk repeats the walk of k_walk_soft (same Philox draws, the
+// same exact nearest primitives, so the same positions), keeping each step's
+// position, primitive and throughput in `state` / `sbeta` (step-major, so a
+// step's stores coalesce), then sweeps the steps backwards applying the
+// transposes of the step relations of k_walk_soft's tangent recurrence:
+//   res  += [d > 0] beta (1 - w) g,   beta *= w,   w = min(d, eps) / eps,
+//   p    += dir d (before the next step),
+// with the tangents dd = n.(pd - cd) and gd of soft_tangents.
+template <int D, bool BVH>
+__global__ void __launch_bounds__(128) k_soft_adjoint(SceneView S, WalkCfg c, const float *__restrict__ P,
+                                                      long long w0, long long nchunk,
+                                                      const float *__restrict__ dLdu, float4 *state, float *sbeta,
+                                                      double *dV, double *dg) {
+    const float eps = c.eps;
+    for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < nchunk;
+         l += (long long)gridDim.x * blockDim.x) {
+        const long long idx = w0 + l;
+        const uint32_t pt = (uint32_t)(idx / c.nwalks);
+        const uint32_t wk = c.walk_offset + (uint32_t)(idx - (long long)pt * c.nwalks);
+        const float W = dLdu[pt] / (float)c.nwalks;
+        if (W == 0.0f) continue;
+        float p[3];
+        walk_origin<D>(c, P, pt, wk, p);
+        Work work{0, 0, 0};
+        float beta = 1.0f;
+        bool ok = true;
+        for (int i = 0; i < c.nsteps; ++i) {
+            const Hit hit = query<D, BVH>(S, p, nullptr, 0, work);
+            if (hit.prim < 0 || (i == 0 && !c.double_sided && !inside_test<D>(S, p, hit, nullptr))) {
+                ok = false;  // the walk's value is 0 (k_walk_soft): no derivative
+                break;
+            }
+            state[(size_t)i * nchunk + l] = make_float4(p[0], p[1], D == 3 ? p[2] : 0.0f, __int_as_float(hit.prim));
+            sbeta[(size_t)i * nchunk + l] = beta;
+            const float d = sqrtf(hit.d2);
+            beta = beta * (fminf(d, eps) / eps);
+            if (i == c.nsteps - 1) break;
+            float dir[3];
+            soft_dir<D>(c, pt, wk, i, dir);
+            for (int k = 0; k < D; ++k) p[k] = fmaf(dir[k], d, p[k]);
+        }
+        if (!ok) continue;
+        float pbar[3] = {0.0f, 0.0f, 0.0f};  // adjoint of the position tangent entering the step
+        float bbar = 0.0f;                   // adjoint of the throughput tangent entering the step
+        for (int i = c.nsteps - 1; i >= 0; --i) {
+            const float4 sv = state[(size_t)i * nchunk + l];
+            const float x[3] = {sv.x, sv.y, sv.z};
+            const int prim = __float_as_int(sv.w);
+            const float bt = sbeta[(size_t)i * nchunk + l];
+            const float d = sqrtf(prim_d2<D>(S, prim, x));
+            const Rec r = closest_record<D>(S, x, prim);
+            int vid[3];
+            float wts[3];
+            const float g = dirichlet<D>(S, prim, r.t0, r.t1, vid, wts);
+            const float w = fminf(d, eps) / eps;
+            float dbar = 0.0f;
+            if (i < c.nsteps - 1) {
+                // p_{i+1} = p_i + dir d: the next step's position adjoint flows into d
+                float dir[3];
+                soft_dir<D>(c, pt, wk, i, dir);
+                for (int k = 0; k < D; ++k) dbar += pbar[k] * dir[k];
+            }
+            const bool contrib = d > 0.0f;
+            const float gbar = contrib ? W * bt * (1.0f - w) : 0.0f;
+            const float wbar = (contrib ? -W * bt * g : 0.0f) + bbar * bt;
+            if (d < eps) dbar += wbar / eps;
+            bbar = (contrib ? W * (1.0f - w) * g : 0.0f) + bbar * w;
+            // dd = n.(pd - cd), n = (x - c) / d, cd = sum_j wts_j dV_j
+            if (d > 0.0f && dbar != 0.0f) {
+                for (int k = 0; k < D; ++k) {
+                    const float nk = (x[k] - r.p[k]) / d;
+                    pbar[k] += dbar * nk;
+                    for (int j = 0; j < D; ++j)
+                        atomicAdd(&dV[(size_t)vid[j] * D + k], (double)(-dbar * nk * wts[j]));
+                }
+            }
+            // gd = sum_j bd_j g_j + sum_j wts_j dg_j
+            if (gbar != 0.0f) {
+                if (dg != nullptr)
+                    for (int j = 0; j < D; ++j) atomicAdd(&dg[vid[j]], (double)(gbar * wts[j]));
+                soft_bary_adjoint<D>(S, x, r, prim, vid, gbar, pbar, dV);
+            }
+        }
+    }
+}
+
+template <int D, bool BVH>
+static int launch_soft_adjoint_t(const SceneImpl &S, const float *P, long long total, const wos_params &p,
+                                 const float *dLdu, double *dV, double *dg, cudaStream_t st) {
+    const SceneView v = S.view();
+    const WalkCfg c = make_cfg(p);
+    // walks per chunk: the per-step state (20 B per walk and step) stays under 256 MB
+    const long long per_walk = (long long)p.nsteps * (long long)(sizeof(float4) + sizeof(float));
+    const long long chunk = std::max(1LL, std::min(total, (256LL << 20) / per_walk));
+    float4 *state = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&state, (size_t)(chunk * per_walk), st);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMallocAsync(soft adjoint state)");
+    float *sbeta = reinterpret_cast<float *>(state + (size_t)chunk * p.nsteps);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    for (long long w0 = 0; w0 < total && e == cudaSuccess; w0 += chunk) {
+        const long long nc = std::min(chunk, total - w0);
+        const int grid = (int)std::min<long long>((nc + 127) / 128, (long long)sms * 16);
+        k_soft_adjoint<D, BVH><<<grid, 128, 0, st>>>(v, c, P, w0, nc, dLdu, state, sbeta, dV, dg);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(state, st);
+    if (e != cudaSuccess) return fail_cuda(e, "k_soft_adjoint launch");
+    return 0;
+}
+
+int launch_soft_adjoint(const SceneImpl &S, const float *P, long long total, const wos_params &p, const float *dLdu,
+                        double *dV, double *dg, cudaStream_t st) {
+    if (total == 0) return 0;
+    const bool bvh = p.use_bvh != 0;
+    if (S.dim == 2)
+        return bvh ? launch_soft_adjoint_t<2, true>(S, P, total, p, dLdu, dV, dg, st)
+                   : launch_soft_adjoint_t<2, false>(S, P, total, p, dLdu, dV, dg, st);
+    return bvh ? launch_soft_adjoint_t<3, true>(S, P, total, p, dLdu, dV, dg, st)
+               : launch_soft_adjoint_t<3, false>(S, P, total, p, dLdu, dV, dg, st);
+}
+
 template <int D, bool BVH, int WL>
 static int launch_soft_t(const SceneImpl &S, const float *P, long long total, const wos_params &p, const float *tV,
                          const float *tg, float *vals, float *tans, unsigned long long *counter, cudaStream_t st) {

@@ -119,6 +119,8 @@ int launch_walk_soft(const SceneImpl &S, const float *P, long long total, const 
 int launch_walk_plain(const SceneImpl &S, const float *P, long long total, const wos_params &p, float *values,
                       cudaStream_t st);
 int launch_reduce(const float *vals, int n, int nw, double *mean, double *var, cudaStream_t st);
+int launch_soft_adjoint(const SceneImpl &S, const float *P, long long total, const wos_params &p, const float *dLdu,
+                        double *dV, double *dg, cudaStream_t st);
 int launch_closest(const SceneImpl &S, const float *P, int n, bool bvh, const QueryOut &o, cudaStream_t st);
 int launch_ball(const SceneImpl &S, const uint8_t *valid, const float *pt, const float *nrm, int n, float eps,
                 bool bvh, float *R, cudaStream_t st);

@@ -158,6 +158,7 @@ SIGNATURES = {
     "wos_solve_adjoint_workspace_size": (_S, [_P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams)]),
     "wos_soft_walk_workspace_size": (_S, [_I, ctypes.POINTER(WosParams)]),
     "wos_soft_walk": (_I, [_P, _P, _I, ctypes.POINTER(WosParams), _P, _P, _P, _P, _P, _P, _P, _S, _P]),
+    "wos_soft_walk_adjoint": (_I, [_P, _P, _I, ctypes.POINTER(WosParams), _P, _P, _P, _P]),
     "wos_boundary_term": (_I, [_P, ctypes.POINTER(WosDetector), _I, ctypes.c_uint64, _P, _P, _P, _P, _P]),
     "wos_solve_tangent_workspace_size": (_S, [_P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams)]),
     "wos_solve_tangent": (

@@ -346,6 +346,24 @@ class NativeScene:
                  _ptr(var), _ptr(tan), _ptr(tvar), ws.data_ptr(), need, stream())
         return dict(mean=mean, var=var, tangent=tan, tangent_var=tvar)
 
+    def soft_walk_adjoint(self, P, s: WalkSettings, dLdu, want_dV=True, want_dg=True):
+        """Reverse mode of the soft-edge walk (wos_soft_walk_adjoint): the
+        gradients of sum_i dLdu[i] mean_i with respect to the vertices and the
+        values (None where not wanted)."""
+        P = as_cuda(P, torch.float32, self.dim)
+        dLdu = as_cuda(dLdu, torch.float32).reshape(-1)
+        n = int(P.shape[0])
+        if dLdu.numel() != n:
+            raise ValueError("dLdu must have one entry per point")
+        d = self.device
+        dV = torch.zeros((self.nV, self.dim), dtype=torch.float32, device=d) if want_dV else None
+        dg = torch.zeros(self.nV, dtype=torch.float32, device=d) if want_dg else None
+        if n and (want_dV or want_dg):
+            c = s.c()
+            call("wos_soft_walk_adjoint", self.h, P.data_ptr(), n, ctypes.byref(c), dLdu.data_ptr(), _ptr(dV),
+                 _ptr(dg), stream())
+        return dV, dg
+
     def boundary_term(self, det, nwalks: int, seed: int = 0, dV_dir=None, dLdI=None):
         """Image-space boundary term (wos_boundary_term): the derivative image
         for vertex motion dV_dir (forward mode) and / or the vertex gradient

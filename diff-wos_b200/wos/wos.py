@@ -59,8 +59,11 @@ class WoSCUDA(WoS):
 
 
 class _SoftFunction(torch.autograd.Function):
-    """Per-point means of the soft-edge walk, differentiable in forward mode
-    (the reference's renderD use of Baseline, diff_solve/runner.py:75-109)."""
+    """Per-point means of the soft-edge walk, differentiable in both modes:
+    forward mode (the reference's renderD use of Baseline,
+    diff_solve/runner.py:75-109) by wos_soft_walk's tangents, reverse mode by
+    wos_soft_walk_adjoint (the reference's walk is a fully attached Dr.Jit
+    computation, wos/wos.py:170-187)."""
 
     @staticmethod
     def forward(ctx, solver, scene, P, s, vertices, values):
@@ -73,9 +76,11 @@ class _SoftFunction(torch.autograd.Function):
         return out["tangent"].to(torch.float32)
 
     @staticmethod
+    @torch.autograd.function.once_differentiable
     def backward(ctx, grad):
-        raise NotImplementedError("the soft-edge baseline is differentiated in forward mode only "
-                                  "(torch.autograd.forward_ad); use OursCUDA for reverse mode")
+        need_V, need_g = ctx.needs_input_grad[4], ctx.needs_input_grad[5]
+        dV, dg = ctx.scene._native.soft_walk_adjoint(ctx.P, ctx.s, grad, want_dV=need_V, want_dg=need_g)
+        return None, None, None, None, dV, dg
 
 
 class _SoftWalk:

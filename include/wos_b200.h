@@ -312,6 +312,17 @@ WOS_API int wos_soft_walk(wos_scene_t scene, const float *P, int n, const wos_pa
                           const float *dg_dir, double *mean, double *var, double *tangent, double *tangent_var,
                           void *workspace, size_t workspace_bytes, wos_stream_t stream);
 
+/* Reverse mode of wos_soft_walk (the Baseline / Baseline3D walks are fully
+ * attached in the reference, wos/wos.py:170-187, wos/wos_grad_3d.py:39-57, so
+ * Dr.Jit differentiates them in either mode): dV (nV x dim) and dg (nV),
+ * float32 device arrays that are ADDED to (either may be NULL), receive
+ * sum_i dLdu[i] d mean_i / d(vertices, values) over the same walks as
+ * wos_soft_walk with the same params.  Each walk is repeated from its Philox
+ * counters and its per-step positions are kept in scratch memory allocated
+ * stream-ordered (at most 256 MB at a time; walks are processed in chunks). */
+WOS_API int wos_soft_walk_adjoint(wos_scene_t scene, const float *P, int n, const wos_params *p, const float *dLdu,
+                                  float *dV, float *dg, wos_stream_t stream);
+
 /* A detector: res[0] x res[1] pixels over [vmin, vmax] in scene axes
  * (axis_u, axis_v); in 3D a slab |x[slab_axis] - slab_center| <
  * slab_half_width (slab_axis -1 in 2D); size = its area (2D) or slab volume

@@ -4,6 +4,8 @@ of diff-wos inv_solve, seed = iteration).  The loss must fall by a large
 factor and the recovered values must approach the truth."""
 from __future__ import annotations
 
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -83,4 +85,64 @@ def test_inverse_translation_converges(cuda):
     t_avg = torch.stack(tail).mean(0)
     err = float(torch.linalg.norm(t_avg - t_true))
     assert err < 0.008, (t_avg.cpu().numpy(), err)
+    assert wos.device_status() == 0
+
+
+def _wrench_in_box(angle, shift):
+    """inv_solve/test_wrench.py:54-66: the wrench (data/meshes/wrench.obj,
+    flipped) rotated by `angle` and shifted, concatenated with the script's
+    box polyline (its four corners as written there, the fourth repeating the
+    second) scaled by 5, whose values are 0."""
+    import torch
+    from wos import io
+    V, F, g = io.read_2d_obj(Path(__file__).resolve().parent / "golden" / "meshes" / "wrench.obj",
+                             flip_orientation=True)
+    V0 = torch.tensor(V, dtype=torch.float32, device="cuda")
+    c, s = torch.cos(angle), torch.sin(angle)
+    R = torch.stack([torch.stack([c, -s]), torch.stack([s, c])])
+    shape = V0 @ R.T + shift
+    box = torch.tensor([[-1.0, -1.0], [-1.0, 1.0], [1.0, 1.0], [-1.0, 1.0]], device="cuda") * 5.0
+    verts = torch.cat([shape, box])
+    faces = np.concatenate([F, np.array([[0, 1], [1, 2], [2, 3], [3, 0]]) + len(V)]).astype(np.int32)
+    values = torch.cat([torch.tensor(g, dtype=torch.float32, device="cuda"), torch.zeros(4, device="cuda")])
+    return verts, faces, values
+
+
+def test_wrench_rotation_in_box_converges(cuda):
+    """The reference's scene-transform inverse problem (inv_solve/test_wrench.py:
+    12-115): observations on the boundary of [-1, 1]^2 (a 1024 grid's border,
+    4,092 points), double-sided walks, L1 loss, Adam with lr 0.06 on the
+    rotation and 1e-5 on the translation, the forward WoSCUDA with 100 walks
+    and the gradient from OursCUDA with 10 walks, epsilon2 5e-4, clamping 0.1;
+    the target rotation is pi / 2 from a start at 0."""
+    import torch
+    import wos
+    x = np.linspace(-1.0, 1.0, 1024)
+    X, Y = np.meshgrid(x, x)
+    m = np.abs(np.maximum(np.abs(X), np.abs(Y)) - 1.0) < 1e-4
+    Pd = torch.tensor(np.stack([X[m], Y[m]], 1), dtype=torch.float32, device="cuda")
+    assert len(Pd) == 4092
+    tgt = wos.Polyline(*_wrench_in_box(torch.tensor(np.pi / 2, device="cuda"), torch.zeros(2, device="cuda")))
+    target = wos.WoSCUDA(nwalks=10000, nsteps=64, double_sided=True).solve(Pd, tgt, seed=12345)
+    rot = torch.zeros((), device="cuda", requires_grad=True)
+    shift = torch.zeros(2, device="cuda", requires_grad=True)
+    opt = torch.optim.Adam([rot], lr=0.06)
+    opt2 = torch.optim.Adam([shift], lr=1e-5)
+    solver = wos.CustomSolver(wos.WoSCUDA(nwalks=100, nsteps=64, double_sided=True),
+                              wos.OursCUDA(nwalks=10, nsteps=64, double_sided=True, epsilon2=5e-4, clamping=0.1))
+    losses, rots = [], []
+    for it in range(200):
+        scene = wos.Polyline(*_wrench_in_box(rot, shift))
+        u = solver.walk(Pd, scene, seed=it)
+        loss = (u - target).abs().sum()
+        opt.zero_grad()
+        opt2.zero_grad()
+        loss.backward()
+        opt.step()
+        opt2.step()
+        losses.append(float(loss))
+        rots.append(float(rot))
+    final = float(np.mean(rots[-20:]))
+    assert abs(final - np.pi / 2) < 0.05, (final, rots[::20])
+    assert np.mean(losses[-20:]) < 0.25 * losses[0], (losses[0], losses[-20:])
     assert wos.device_status() == 0

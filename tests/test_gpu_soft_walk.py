@@ -1,6 +1,7 @@
 """The soft-edge walk of Baseline / Baseline3D: values against the oracle,
 forward-mode derivatives against central finite differences with common
-random numbers, and torch forward AD through Baseline.walk_detector."""
+random numbers, reverse mode against forward mode and finite differences, and
+torch forward and reverse AD through Baseline."""
 from __future__ import annotations
 
 import numpy as np
@@ -94,6 +95,82 @@ def test_baseline_forward_ad_walk_detector(cuda):
     P = _np(det.make_points())
     inside = np.hypot(P[:, 0], P[:, 1]) < 0.6
     assert abs(float(np.mean(_np(tan)[inside] + 2 * P[inside, 0]))) < 0.05
-    with pytest.raises(NotImplementedError):
-        Vr = torch.tensor(V, device="cuda", requires_grad=True)
-        solver.walk(P, wos.Polyline(Vr, F, torch.tensor(g, device="cuda")), seed=1).sum().backward()
+    # reverse mode through torch autograd is the native adjoint
+    Vr = torch.tensor(V, device="cuda", requires_grad=True)
+    gr = torch.tensor(g, device="cuda", requires_grad=True)
+    scene_r = wos.Polyline(Vr, F, gr)
+    w = torch.tensor(np.random.default_rng(3).normal(size=len(P)).astype(np.float32), device="cuda")
+    (solver.walk(P, scene_r, seed=1) * w).sum().backward()
+    dV, dg = scene_r._native.soft_walk_adjoint(P, solver.soft_settings(scene_r, 1), w)
+    np.testing.assert_allclose(_np(Vr.grad), _np(dV), rtol=1e-6, atol=1e-7)
+    np.testing.assert_allclose(_np(gr.grad), _np(dg), rtol=1e-6, atol=1e-7)
+
+
+
+def _soft_case(dim, rng):
+    from wos import shapes
+    if dim == 2:
+        V, F = shapes.star(96, 0.6, 0.2, 4)
+        P = rng.uniform(-0.35, 0.35, (256, 2)).astype(np.float32)
+    else:
+        V, F = shapes.displaced_icosphere(2, 0.1, seed=2)
+        P = rng.uniform(-0.35, 0.35, (128, 3)).astype(np.float32)
+    g = (V[:, 0] ** 2 - V[:, 1] ** 2 + 0.5 * V[:, 0]).astype(np.float32)
+    return V, F, g, P
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("use_bvh", [True, False])
+def test_soft_walk_reverse_equals_forward(cuda, dim, use_bvh):
+    """wos_soft_walk_adjoint is the transpose of the tangent recurrence: for
+    point weights w and any direction, <adjoint(w), direction> =
+    sum_i w_i tangent_i (FP64 sums of float32 walk terms)."""
+    import torch
+    import wos
+    from wos.native import NativeScene, WalkSettings
+    rng = np.random.default_rng(5)
+    V, F, g, P = _soft_case(dim, rng)
+    ns = NativeScene(V, F, g)
+    s = WalkSettings(nwalks=32, nsteps=24, epsilon=2e-2, seed=13, use_bvh=use_bvh)
+    dirV = torch.tensor(rng.normal(size=V.shape).astype(np.float32), device="cuda")
+    dirg = torch.tensor(rng.normal(size=len(V)).astype(np.float32), device="cuda")
+    w = torch.tensor(rng.normal(size=len(P)).astype(np.float32), device="cuda")
+    t = ns.soft_walk(P, s, dV=dirV, dg=dirg, want_tangent=True)
+    dV, dg = ns.soft_walk_adjoint(P, s, w)
+    lhs = float((w.double() * t["tangent"]).sum())
+    rhs = float((dV.double() * dirV.double()).sum() + (dg.double() * dirg.double()).sum())
+    scale = float((w.abs().double() * t["tangent"].abs()).sum())
+    assert abs(lhs - rhs) <= 1e-4 * scale, (lhs, rhs, scale)
+    # each part alone
+    tV = ns.soft_walk(P, s, dV=dirV, want_tangent=True)["tangent"]
+    assert abs(float((w.double() * tV).sum()) - float((dV.double() * dirV.double()).sum())) <= 1e-4 * scale
+    assert wos.device_status() == 0
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_soft_walk_reverse_matches_finite_differences(cuda, dim):
+    """The vertex gradient of L = sum_i w_i mean_i along a seeded direction
+    against central finite differences with common random numbers, over 16
+    seeds: within 2 standard errors."""
+    import torch
+    from wos.native import NativeScene, WalkSettings
+    rng = np.random.default_rng(6)
+    V, F, g, P = _soft_case(dim, rng)
+    dirV = rng.normal(size=V.shape).astype(np.float32) * 0.2
+    dirV[:, 0] += 1.0
+    w = torch.tensor(rng.uniform(0.5, 1.5, len(P)).astype(np.float32), device="cuda")
+    ns = NativeScene(V, F, g)
+    h = 5e-5
+    plus, minus = NativeScene(V + h * dirV, F, g), NativeScene(V - h * dirV, F, g)
+    adj, fd = [], []
+    for seed in range(16):
+        s = WalkSettings(nwalks=64, nsteps=8, epsilon=5e-2, seed=100 + seed)
+        dV, _ = ns.soft_walk_adjoint(P, s, w, want_dg=False)
+        adj.append(float((dV.double() * torch.tensor(dirV, device="cuda").double()).sum()))
+        lp = float((w.double() * plus.soft_walk(P, s)["mean"]).sum())
+        lm = float((w.double() * minus.soft_walk(P, s)["mean"]).sum())
+        fd.append((lp - lm) / (2 * h))
+    adj, fd = np.array(adj), np.array(fd)
+    se = np.sqrt(adj.var(ddof=1) / len(adj) + fd.var(ddof=1) / len(fd))
+    z = (adj.mean() - fd.mean()) / se
+    assert abs(z) < 2.0, (adj.mean(), fd.mean(), se)
