@@ -329,9 +329,9 @@ int wos_solve(wos_scene_t scene, const float *P, int n, const wos_params *p, dou
     return launch_reduce(vals, n, p->nwalks, mean, var, st);
 }
 
-int wos_normal_derivative(wos_scene_t scene, const uint8_t *valid, const float *pt, const float *normal,
-                          const float *t_or_uv, const int32_t *prim, int n, const wos_params *p,
-                          const wos_adjoint_params *a, float *out, wos_stream_t stream) {
+static int normal_derivative_impl(wos_scene_t scene, const uint8_t *valid, const float *pt, const float *normal,
+                                  const float *t_or_uv, const int32_t *prim, const float *R, int n, const wos_params *p,
+                                  const wos_adjoint_params *a, float *out, wos_stream_t stream) {
     if (scene == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "scene is NULL");
     if (int rc = check_params(p)) return rc;
     if (int rc = check_adj(a)) return rc;
@@ -342,6 +342,7 @@ int wos_normal_derivative(wos_scene_t scene, const uint8_t *valid, const float *
     WOS_CHECK_DEV(normal, "normal");
     WOS_CHECK_DEV(t_or_uv, "t_or_uv");
     WOS_CHECK_DEV(prim, "prim");
+    WOS_CHECK_DEV_OPT(R, "R");
     WOS_CHECK_DEV(out, "out");
     cudaStream_t st = (cudaStream_t)stream;
     Scratch s;
@@ -352,9 +353,23 @@ int wos_normal_derivative(wos_scene_t scene, const uint8_t *valid, const float *
     o.rnrm = normal;
     o.rtuv = t_or_uv;
     o.rprim = prim;
+    o.rR = R;
     o.nd = out;
     return launch_adjoint(scene->impl, nullptr, n, *p, make_adj(*a), nullptr, ADJ_ND_ONLY, o, (unsigned long long *)s.base,
                           st);
+}
+
+int wos_normal_derivative(wos_scene_t scene, const uint8_t *valid, const float *pt, const float *normal,
+                          const float *t_or_uv, const int32_t *prim, int n, const wos_params *p,
+                          const wos_adjoint_params *a, float *out, wos_stream_t stream) {
+    return normal_derivative_impl(scene, valid, pt, normal, t_or_uv, prim, nullptr, n, p, a, out, stream);
+}
+
+int wos_normal_derivative_radius(wos_scene_t scene, const uint8_t *valid, const float *pt, const float *normal,
+                                 const float *t_or_uv, const int32_t *prim, const float *R, int n,
+                                 const wos_params *p, const wos_adjoint_params *a, float *out, wos_stream_t stream) {
+    if (R == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "R is NULL");
+    return normal_derivative_impl(scene, valid, pt, normal, t_or_uv, prim, R, n, p, a, out, stream);
 }
 
 size_t wos_adjoint_workspace_size(wos_scene_t scene) {

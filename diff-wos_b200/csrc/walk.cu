@@ -889,6 +889,14 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
                 }
             }
         }
+        if (active && phase == PH_ND_START && out.rR != nullptr) {
+            // a given ball radius (override_R, wos/wos.py:71-74): no bisection
+            st.uref = dirichlet<D>(S, rprim, rt0, rt1, nullptr, nullptr);
+            st.R = out.rR[pt];
+            nd_setup<D>(st, S, c, a, pt, wk);
+            nd_point<D>(st, qpos);
+            phase = PH_ANTI_START;
+        }
         if (active && phase == PH_ND_START) {
             // no query needed to start: set up the bisection
             st.uref = dirichlet<D>(S, rprim, rt0, rt1, nullptr, nullptr);

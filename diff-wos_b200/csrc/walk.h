@@ -51,6 +51,7 @@ struct AdjOut {
     const uint8_t *rvalid;
     const float *rpt, *rnrm, *rtuv;
     const int *rprim;
+    const float *rR;  // given ball radii (override_R), or null: the inscribed ball
     float *nd;
     // records mode: per-walk WalkRec and source derivatives from the forward pass
     const int *wrec;

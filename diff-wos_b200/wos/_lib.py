@@ -143,6 +143,10 @@ SIGNATURES = {
         _I,
         [_P, _P, _P, _P, _P, _P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams), _P, _P],
     ),
+    "wos_normal_derivative_radius": (
+        _I,
+        [_P, _P, _P, _P, _P, _P, _P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams), _P, _P],
+    ),
     "wos_adjoint_workspace_size": (_S, [_P]),
     "wos_adjoint": (
         _I,

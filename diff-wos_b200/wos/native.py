@@ -383,7 +383,9 @@ class NativeScene:
              _ptr(img), _ptr(w), _ptr(dV), stream())
         return img, dV
 
-    def normal_derivative(self, rec, s: WalkSettings, a: AdjointSettings) -> torch.Tensor:
+    def normal_derivative(self, rec, s: WalkSettings, a: AdjointSettings, R=None) -> torch.Tensor:
+        """One normal-derivative estimate per record (grad * outward normal);
+        R: per-record ball radii (override_R), default the inscribed ball."""
         valid = as_cuda(rec["valid"], torch.uint8).reshape(-1)
         n = int(valid.numel())
         out = torch.empty((n, self.dim), dtype=torch.float32, device=self.device)
@@ -393,8 +395,18 @@ class NativeScene:
             tuv = as_cuda(rec["tuv"], torch.float32, 2)
             prim = as_cuda(rec["prim"], torch.int32).reshape(-1)
             c, ca = s.c(), a.c()
-            call("wos_normal_derivative", self.h, valid.data_ptr(), pt.data_ptr(), nrm.data_ptr(), tuv.data_ptr(),
-                 prim.data_ptr(), n, ctypes.byref(c), ctypes.byref(ca), out.data_ptr(), stream())
+            if R is None:
+                call("wos_normal_derivative", self.h, valid.data_ptr(), pt.data_ptr(), nrm.data_ptr(),
+                     tuv.data_ptr(), prim.data_ptr(), n, ctypes.byref(c), ctypes.byref(ca), out.data_ptr(), stream())
+            else:
+                Rt = as_cuda(R, torch.float32).reshape(-1)
+                if Rt.numel() == 1:
+                    Rt = Rt.expand(n).contiguous()
+                if Rt.numel() != n:
+                    raise ValueError("R must be a scalar or have one entry per record")
+                call("wos_normal_derivative_radius", self.h, valid.data_ptr(), pt.data_ptr(), nrm.data_ptr(),
+                     tuv.data_ptr(), prim.data_ptr(), Rt.data_ptr(), n, ctypes.byref(c), ctypes.byref(ca),
+                     out.data_ptr(), stream())
         return out
 
     def adjoint(self, P, s: WalkSettings, a: AdjointSettings, dLdu, workspace: torch.Tensor | None = None):

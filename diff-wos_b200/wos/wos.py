@@ -27,17 +27,16 @@ class WoS(Solver):
 
     def normal_derivative(self, its, scene, sampler, override_R=None, clamping=1e-1, control_variates=True):
         """du/dn at boundary records (wos/wos.py:59-107): off-centred Poisson
-        kernel on the largest inscribed ball, two antithetic samples, each a
-        full walk at this solver's epsilon.  Returns (grad * n_x, grad * n_y)
-        with n the outward normal."""
-        if override_R is not None:
-            raise NotImplementedError("override_R is not supported; the ball radius is always the inscribed one")
+        kernel on the largest inscribed ball (or on balls of radius override_R,
+        a scalar or one per record), two antithetic samples, each a full walk
+        at this solver's epsilon.  Returns (grad * n_x, grad * n_y) with n the
+        outward normal."""
         s = as_sampler(sampler)
         st = self.walk_settings(scene, s.seed, nwalks=1, walk_offset=s.take())
         a = AdjointSettings(epsilon2=float(self.epsilon), clamping=float(clamping),
                             control_variates=bool(control_variates),
                             source_in_normal_derivative=bool(self.source_in_normal_derivative))
-        out = scene._native.normal_derivative(its.as_dict(), st, a)
+        out = scene._native.normal_derivative(its.as_dict(), st, a, R=override_R)
         return tuple(out[:, k] for k in range(scene.dim))
 
     def tangent_derivative(self, its, scene, sampler=None):

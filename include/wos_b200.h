@@ -221,6 +221,15 @@ WOS_API int wos_normal_derivative(wos_scene_t scene, const uint8_t *valid, const
                           const float *t_or_uv, const int32_t *prim, int n, const wos_params *p,
                           const wos_adjoint_params *a, float *out, wos_stream_t stream);
 
+/* wos_normal_derivative on balls of given radii R (n floats, device) instead
+ * of the largest inscribed ball: WoS.normal_derivative(..., override_R=R)
+ * (wos/wos.py:59-107, override_R at :71-74; wos/wos_with_source.py:167-172).
+ * The ball of record i is centred at pt - n_out R[i]. */
+WOS_API int wos_normal_derivative_radius(wos_scene_t scene, const uint8_t *valid, const float *pt, const float *normal,
+                                         const float *t_or_uv, const int32_t *prim, const float *R, int n,
+                                         const wos_params *p, const wos_adjoint_params *a, float *out,
+                                         wos_stream_t stream);
+
 /* Workspace bytes for wos_adjoint on this scene. */
 WOS_API size_t wos_adjoint_workspace_size(wos_scene_t scene);
 

@@ -134,6 +134,8 @@ def lib() -> ctypes.CDLL:
         L.orc_soft_walk.argtypes = [P, P, I, ctypes.POINTER(Params), P, I]
         L.orc_adjoint_counted.argtypes = [P, P, I, ctypes.POINTER(Params), ctypes.POINTER(AdjParams), P, P, P, P, I,
                                           P]
+        L.orc_normal_derivative_r.argtypes = [P, P, P, P, P, P, P, I, ctypes.POINTER(Params),
+                                              ctypes.POINTER(AdjParams), P, I]
         L.orc_boundary_term.argtypes = [P, ctypes.POINTER(Detector), I, ctypes.c_uint64, P, P, P, P, I]
         _lib = L
     return _lib
@@ -249,12 +251,14 @@ class OracleScene:
                                _p(out["n"]), _p(out["tuv"]), _p(out["prim"]), _p(out["contrib"]), nthreads)
         return out
 
-    def normal_derivative(self, rec, params: Params, adj: AdjParams, nthreads=0):
+    def normal_derivative(self, rec, params: Params, adj: AdjParams, nthreads=0, R=None):
+        """One estimate per record; R: per-record ball radii (override_R)."""
         n = rec["valid"].shape[0]
         out = np.zeros((n, self.dim), np.float32)
-        lib().orc_normal_derivative(self.h, _p(np.ascontiguousarray(rec["valid"], np.uint8)), _p(_f32(rec["pt"])),
-                                    _p(_f32(rec["n"])), _p(_f32(rec["tuv"])), _p(_i32(rec["prim"])), n,
-                                    ctypes.byref(params), ctypes.byref(adj), _p(out), nthreads)
+        Rv = None if R is None else np.ascontiguousarray(np.broadcast_to(np.asarray(R, np.float32), (n,)))
+        lib().orc_normal_derivative_r(self.h, _p(np.ascontiguousarray(rec["valid"], np.uint8)), _p(_f32(rec["pt"])),
+                                      _p(_f32(rec["n"])), _p(_f32(rec["tuv"])), _p(_i32(rec["prim"])), _p(Rv), n,
+                                      ctypes.byref(params), ctypes.byref(adj), _p(out), nthreads)
         return out
 
     def adjoint(self, P, params: Params, adj: AdjParams, dLdu, nthreads=0):

@@ -894,7 +894,7 @@ static inline float eval_P(const float *c, const float *y, const float *s, float
 
 // Normal-derivative estimate at a boundary record; returns grad * n_out.
 static void normal_derivative(const Scene &S, const Rec &rec, const Params &prm, const AdjParams &ap,
-                              const Rng &rng, uint32_t pt, uint32_t wk, float *out) {
+                              const Rng &rng, uint32_t pt, uint32_t wk, float *out, const float *R_given = nullptr) {
     const int D = S.D;
     const bool bvh = prm.use_bvh != 0;
     const bool with_src = ap.source_in_normal_derivative && S.src_type != 0 && D == 2;
@@ -904,7 +904,8 @@ static void normal_derivative(const Scene &S, const Rec &rec, const Params &prm,
         p[k] = rec.p[k];
     }
     const float u_ref = dirichlet(S, rec);
-    const float R = inscribed_ball(S, rec, ap.ball_epsilon, bvh);
+    // the largest inscribed ball, or a given radius (override_R, wos/wos.py:71-74)
+    const float R = R_given != nullptr ? *R_given : inscribed_ball(S, rec, ap.ball_epsilon, bvh);
     float c[3];
     for (int k = 0; k < D; ++k) c[k] = fmaf(-n[k], R, p[k]);
     const U4 rx = rng.draw(pt, wk, 0, ROLE_EXTRA);
@@ -1546,8 +1547,9 @@ void orc_reduce(const float *vals, int n, int nwalks, double *mean, double *var)
 
 // Normal-derivative estimates at records (one sample per record, walk index
 // prm->walk_offset); out = grad * n_out, n x dim.
-void orc_normal_derivative(void *s, const unsigned char *valid, const float *pt, const float *nrm, const float *tuv,
-                           const int *prim, int n, const Params *prm, const AdjParams *ap, float *out, int nthreads) {
+void orc_normal_derivative_r(void *s, const unsigned char *valid, const float *pt, const float *nrm, const float *tuv,
+                             const int *prim, const float *R, int n, const Params *prm, const AdjParams *ap, float *out,
+                             int nthreads) {
     Scene *S = (Scene *)s;
     const int D = S->D;
     const Rng rng = make_rng(prm->seed);
@@ -1564,9 +1566,14 @@ void orc_normal_derivative(void *s, const unsigned char *valid, const float *pt,
         r.t[0] = tuv[(size_t)i * 2];
         r.t[1] = tuv[(size_t)i * 2 + 1];
         float g[3] = {0, 0, 0};
-        if (r.valid) normal_derivative(*S, r, *prm, *ap, rng, (uint32_t)i, prm->walk_offset, g);
+        if (r.valid) normal_derivative(*S, r, *prm, *ap, rng, (uint32_t)i, prm->walk_offset, g, R ? &R[i] : nullptr);
         for (int k = 0; k < D; ++k) out[(size_t)i * D + k] = g[k];
     }
+}
+
+void orc_normal_derivative(void *s, const unsigned char *valid, const float *pt, const float *nrm, const float *tuv,
+                           const int *prim, int n, const Params *prm, const AdjParams *ap, float *out, int nthreads) {
+    orc_normal_derivative_r(s, valid, pt, nrm, tuv, prim, nullptr, n, prm, ap, out, nthreads);
 }
 
 // Adjoint of the per-point means: dL/dtheta = sum_i dLdu[i] * du_i/dtheta,

@@ -380,3 +380,22 @@ def test_projected_walk_adjoint_matches_oracle(cuda, oracle, kind):
     orec = os_.walk_records(P, _oparams(oracle, s1))
     nd = _np(ns.normal_derivative(orec, s1, a))
     assert np.array_equal(nd, os_.normal_derivative(orec, _oparams(oracle, s1), oracle.make_adj(1e-3, 0.1)))
+
+
+@pytest.mark.parametrize("kind", ["circle", "sphere"])
+def test_normal_derivative_given_radius_bit_exact(cuda, oracle, kind):
+    """wos_normal_derivative_radius (override_R): with R the inscribed radius
+    it is wos_normal_derivative; with other radii it equals the oracle's."""
+    from wos.native import AdjointSettings
+    V, F, g = {"circle": circle_scene, "sphere": sphere_scene}[kind]()
+    ns, os_ = _scenes(oracle, V, F, g)
+    P = _pts2(400, 19, -0.7, 0.7) if V.shape[1] == 2 else _pts3(300, 19, -0.6, 0.6)
+    s = _settings(nwalks=1, nsteps=64, seed=23)
+    orec = os_.walk_records(P, _oparams(oracle, s))
+    a = AdjointSettings(epsilon2=5e-4, clamping=0.1)
+    R = _np(ns.inscribed_ball(orec["valid"], orec["pt"], orec["n"]))
+    assert np.array_equal(_np(ns.normal_derivative(orec, s, a, R=R)), _np(ns.normal_derivative(orec, s, a)))
+    R2 = (0.5 * R).astype(np.float32)
+    nd = _np(ns.normal_derivative(orec, s, a, R=R2))
+    ond = os_.normal_derivative(orec, _oparams(oracle, s), oracle.make_adj(5e-4, 0.1), R=R2)
+    assert np.array_equal(nd, ond)

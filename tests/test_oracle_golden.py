@@ -137,6 +137,25 @@ def test_oracle_normal_derivative_disk(oracle):
     assert np.all(np.abs(mean - exact) < 5 * se + 0.05), (mean, exact, se)
 
 
+@pytest.mark.parametrize("R", [0.25, 0.6])
+def test_oracle_normal_derivative_given_radius_disk(oracle, R):
+    """override_R (wos/wos.py:71-74): on any ball inside the domain tangent
+    at the boundary point the estimator stays unbiased; the same disk problem
+    as above on balls of radius R instead of the inscribed one."""
+    S = _circle_oracle(oracle, g_fn=lambda V: np.cos(4 * np.arctan2(V[:, 1], V[:, 0])))
+    theta = np.array([0.3, 1.1, 2.5])
+    P = np.stack([0.999 * np.cos(theta), 0.999 * np.sin(theta)], 1).astype(np.float32)
+    c = S.closest(P)
+    n = 4000
+    rec = dict(valid=np.ones(len(P) * n, np.uint8), pt=np.repeat(c["pt"], n, 0), n=np.repeat(c["n"], n, 0),
+               tuv=np.repeat(c["tuv"], n, 0), prim=np.repeat(c["prim"], n, 0))
+    out = S.normal_derivative(rec, oracle.make_params(nsteps=256, seed=5), oracle.make_adj(1e-4, 1e-2), R=R)
+    g = -(out * rec["n"]).sum(1).reshape(len(P), n)
+    mean, se = g.mean(1), g.std(1) / np.sqrt(n)
+    exact = 4 * np.cos(4 * theta)
+    assert np.all(np.abs(mean - exact) < 5 * se + 0.05), (mean, exact, se)
+
+
 def test_oracle_harmonic_3d(oracle):
     """Displaced icosphere, g = x^2 - y^2 + z."""
     from wos import shapes
