@@ -406,58 +406,6 @@ __global__ void k_leaf_data(const unsigned long long *keys, int n, const float4 
     }
 }
 
-// Smallest sphere containing leaf-ordered triangle s as the distance code
-// sees it (vertices a, a + ab, a + ac from ltri): the midpoint of the longest
-// edge when the triangle is right or obtuse, else the circumcentre; computed
-// in double, the centre rounded to float and the radius widened by that
-// rounding and a relative margin, then rounded up.  Any point of the
-// triangle is within the radius of the float centre.
-__global__ void k_leaf_sphere(const float4 *ltri, int n, float4 *lsph) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    const float4 t0 = ltri[3 * s], t1 = ltri[3 * s + 1], t2 = ltri[3 * s + 2];
-    const double A[3] = {t0.x, t0.y, t0.z};
-    const double ab[3] = {t1.x, t1.y, t1.z}, ac[3] = {t2.x, t2.y, t2.z};
-    double B[3], C[3], bc[3];
-    for (int k = 0; k < 3; ++k) {
-        B[k] = A[k] + ab[k];
-        C[k] = A[k] + ac[k];
-        bc[k] = C[k] - B[k];
-    }
-    auto dot = [](const double *u, const double *v) { return u[0] * v[0] + u[1] * v[1] + u[2] * v[2]; };
-    const double la = dot(bc, bc), lb = dot(ac, ac), lc = dot(ab, ab);  // sides opposite A, B, C
-    double c[3];
-    if (la >= lb + lc || lb >= la + lc || lc >= la + lb) {
-        // right or obtuse (or degenerate): centre on the longest edge
-        const double *P = A, *Q = B;
-        if (la >= lb && la >= lc) {
-            P = B;
-            Q = C;
-        } else if (lb >= lc) {
-            P = A;
-            Q = C;
-        }
-        for (int k = 0; k < 3; ++k) c[k] = 0.5 * (P[k] + Q[k]);
-    } else {
-        // circumcentre: A + (|ac|^2 (ab x ac) x ab + |ab|^2 ac x (ab x ac)) / (2 |ab x ac|^2)
-        const double n[3] = {ab[1] * ac[2] - ab[2] * ac[1], ab[2] * ac[0] - ab[0] * ac[2],
-                             ab[0] * ac[1] - ab[1] * ac[0]};
-        const double nn = dot(n, n);
-        const double u[3] = {n[1] * ab[2] - n[2] * ab[1], n[2] * ab[0] - n[0] * ab[2], n[0] * ab[1] - n[1] * ab[0]};
-        const double v[3] = {ac[1] * n[2] - ac[2] * n[1], ac[2] * n[0] - ac[0] * n[2], ac[0] * n[1] - ac[1] * n[0]};
-        for (int k = 0; k < 3; ++k) c[k] = A[k] + (lb * u[k] + lc * v[k]) / (2.0 * nn);
-    }
-    const float cf[3] = {(float)c[0], (float)c[1], (float)c[2]};
-    const double *verts[3] = {A, B, C};
-    double r2 = 0.0;
-    for (int j = 0; j < 3; ++j) {
-        const double d[3] = {verts[j][0] - cf[0], verts[j][1] - cf[1], verts[j][2] - cf[2]};
-        r2 = fmax(r2, dot(d, d));
-    }
-    const double r = sqrt(r2) * (1.0 + 1e-6) + 1e-9 * sqrt(fmax(la, fmax(lb, lc)));
-    lsph[s] = make_float4(cf[0], cf[1], cf[2], __double2float_ru(r));
-}
-
 // Wide-tree leaves.  Leaf i holds Morton positions [WT_LEAF i, WT_LEAF i +
 // WT_LEAF): its box, and its slab bound -- n = the normalised sum of the
 // primitives' unit normals, c = the box centre computed exactly as the query
@@ -670,7 +618,7 @@ static cudaError_t dalloc(T **p, size_t count, cudaStream_t st) {
 }
 
 void SceneImpl::release(cudaStream_t st) {
-    void *ptrs[] = {V, F, N, g, seg, seginv, tri, node, lseg, lseginv, ltri, lsph, lorig, cdf, wt_box, wt_slab, guide};
+    void *ptrs[] = {V, F, N, g, seg, seginv, tri, node, lseg, lseginv, ltri, lorig, cdf, wt_box, wt_slab, guide};
     for (void *p : ptrs)
         if (p) cudaFreeAsync(p, st);
     V = nullptr;
@@ -684,7 +632,6 @@ void SceneImpl::release(cudaStream_t st) {
     lseg = nullptr;
     lseginv = nullptr;
     ltri = nullptr;
-    lsph = nullptr;
     lorig = nullptr;
     cdf = nullptr;
     wt_box = nullptr;
@@ -820,7 +767,6 @@ static int build_geometry(SceneImpl &S, cudaStream_t st) {
         cudaFreeAsync(tmp, st);
     }
     k_leaf_data<D><<<nblk(nF, TB), TB, 0, st>>>(skeys, nF, S.seg, S.seginv, S.tri, S.lseg, S.lseginv, S.ltri, S.lorig);
-    if (D == 3) k_leaf_sphere<<<nblk(nF, TB), TB, 0, st>>>(S.ltri, nF, S.lsph);
 
     // ---- wide tree (levels 1..wt_levels, the top one with <= 32 nodes)
     {
@@ -927,7 +873,6 @@ int SceneImpl::allocate(cudaStream_t st) {
     } else {
         WOS_TRY(dalloc(&tri, (size_t)nF * 3, st));
         WOS_TRY(dalloc(&ltri, (size_t)nF * 3, st));
-        WOS_TRY(dalloc(&lsph, nF, st));
         WOS_TRY(dalloc(&node, (size_t)std::max(nF - 1, 1) * 4, st));
     }
     WOS_TRY(dalloc(&lorig, nF, st));
@@ -981,7 +926,6 @@ SceneView SceneImpl::view() const {
     v.lseg = prim_order == 1 ? seg : lseg;
     v.lseginv = prim_order == 1 ? seginv : lseginv;
     v.ltri = prim_order == 1 ? tri : ltri;
-    v.lsph = lsph;
     v.lorig = lorig;
     for (int k = 0; k < 3; ++k) {
         v.lo[k] = lo[k];

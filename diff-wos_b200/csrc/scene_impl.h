@@ -41,7 +41,6 @@ struct SceneImpl {
     float4 *lseg = nullptr;
     float *lseginv = nullptr;
     float4 *ltri = nullptr;
-    float4 *lsph = nullptr;  // 3D: bounding sphere (centre, radius) of each leaf-ordered triangle
     int *lorig = nullptr;
     float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
     float half_min_extent = 0;

@@ -50,9 +50,6 @@ struct SceneView {
     const float4 *lseg;
     const float *lseginv;
     const float4 *ltri;
-    // 3D: a sphere (centre xyz, radius w) containing each leaf-ordered
-    // triangle as the distance code sees it, radius rounded up
-    const float4 *lsph;
     const int *lorig;
     float lo[3], hi[3];
     float half_min_extent;  // min_k (hi_k - lo_k) / 2
@@ -615,30 +612,10 @@ __device__ __forceinline__ void wdescend(const SceneView &S, const float *q, int
         // pruning cannot change the frontier) so that its latency overlaps it
         mk = __reduce_min_sync(FULL, key);
         if constexpr (L == 1) {
-            const int s = node * WT_LEAF + lane;
-            bool test = s < S.nF;
-            if constexpr (D == 3) {
-                // Skip the exact test of triangles whose bounding sphere lies
-                // beyond the pruning bound (|q - c| - r > sqrt(bound), checked
-                // squared with a 2^-16 relative margin over the float
-                // roundings), and the whole leaf step when that holds for all
-                // 32.  Such a triangle is farther than any candidate the
-                // bound admits, so the result is unchanged.
-                const float sb = sqrtf(wt_bound(best.d2, tol2));
-                if (test) {
-                    const float4 sp = __ldg(&S.lsph[s]);
-                    const float dx = q[0] - sp.x, dy = q[1] - sp.y, dz = q[2] - sp.z;
-                    const float t = sp.w + sb;
-                    test = !(dot3(dx, dy, dz, dx, dy, dz) > t * t * 1.0000152587890625f);
-                }
-                if (!__any_sync(FULL, test)) {
-                    wk.nb += 1;  // a culled leaf costs like a node expansion
-                    continue;
-                }
-            }
             wk.np += 1;
+            const int s = node * WT_LEAF + lane;
             float d2 = INFINITY;
-            if (test) d2 = leaf_d2<D>(S, s, q);
+            if (s < S.nF) d2 = leaf_d2<D>(S, s, q);
             const float m2 = warp_min(d2);
             if (m2 <= best.d2 && m2 < INFINITY) {
                 const unsigned c2 = __ballot_sync(FULL, d2 == m2);
@@ -705,27 +682,11 @@ __device__ __forceinline__ bool wball_descend(const SceneView &S, const float *q
         const int node = first + j;
         mk = __reduce_min_sync(FULL, key);
         if constexpr (L == 1) {
-            const int s = node * WT_LEAF + lane;
-            bool test = s < S.nF;
-            if constexpr (D == 3) {
-                // the bounding-sphere cull of wdescend: a triangle beyond
-                // sqrt(bound) > m cannot block the ball
-                const float sb = sqrtf(bound);
-                if (test) {
-                    const float4 sp = __ldg(&S.lsph[s]);
-                    const float dx = q[0] - sp.x, dy = q[1] - sp.y, dz = q[2] - sp.z;
-                    const float t = sp.w + sb;
-                    test = !(dot3(dx, dy, dz, dx, dy, dz) > t * t * 1.0000152587890625f);
-                }
-                if (!__any_sync(FULL, test)) {
-                    wk.nb += 1;
-                    continue;
-                }
-            }
             wk.np += 1;
+            const int s = node * WT_LEAF + lane;
             float d2 = INFINITY;
-            if (test) d2 = leaf_d2<D>(S, s, q);
-            const unsigned b = __ballot_sync(FULL, test && ball_blocks(d2, m));
+            if (s < S.nF) d2 = leaf_d2<D>(S, s, q);
+            const unsigned b = __ballot_sync(FULL, s < S.nF && ball_blocks(d2, m));
             if (b) {
                 const int src = __ffs(b) - 1;
                 int o = 0;
