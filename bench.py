@@ -297,7 +297,9 @@ def batched_main(args):
     adj = AdjointSettings(epsilon2=1e-3, clamping=0.1, want_dV=True, want_dg=True, want_dsrc=False)
     plan = wos.BatchPlan(items, adj)
     info = plan.info()
-    best, tune = autotune.tune_batch(plan)
+    # per (dimension, phase) slot; large plans time a prefix of each run
+    sample = min(1.0, 0.1 / max(args.scale, 1e-9))
+    slot_best, slot_ms = autotune.tune_batch_slots(plan, sample=sample)
     for _ in range(args.warmup):
         plan.run(use_graph=True)
     torch.cuda.synchronize()
@@ -358,7 +360,8 @@ def batched_main(args):
     # where the step's time goes: forward-only and forward+adjoint plans per dimension
     def plan_ms(sub, adjoint):
         pl = wos.BatchPlan(sub, adjoint)
-        pl.set_launch(best[0], 0, best[1])
+        for (d, ph), shape in slot_best.items():
+            pl.set_launch_slot(d, ph, *shape)
         pl.run(use_graph=True)
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -385,8 +388,14 @@ def batched_main(args):
                    "launch": "one persistent kernel per dimension, tree depth and phase, CUDA graph replay",
                    "l2": "256 MiB buffer written between timed steps (L2 flush)"},
         "walks_per_s": info["walks"] / (ms * 1e-3),
-        "autotuned_launch": {"block_threads": best[0], "chunk": best[1],
-                             "ms": {f"{k[0]}x{k[1]}": v for k, v in tune.items()}},
+        "autotuned_launch": {
+            "sample": sample,
+            "slots": {f"dim{d}_{'walk' if ph == 0 else 'adjoint'}": {
+                "block_threads": b[0], "blocks_per_sm": b[1], "chunk": b[2],
+                "ms": {f"{c[0]}x{c[1]}x{c[2]}": round(v, 3) for c, v in slot_ms[(d, ph)].items()}}
+                for (d, ph), b in slot_best.items()},
+            "note": "candidates: threads per block x blocks per SM (0 = occupancy limit) x walks per queue grab; "
+                    "each slot's launches timed alone"},
         "breakdown": breakdown,
         "plain_forward_points_per_s": plain,
         "plain_forward_by_dim": plain_by_dim,

@@ -59,7 +59,9 @@ struct wos_batch_s {
     std::vector<wosd::BatchGroup> groups;
     wos_adjoint_params adj{};
     int want_adjoint = 1;
-    wosd::BatchLaunch launch{256, 0, 64, 0};
+    // launch shape per (dimension - 2, phase 0 walk / 1 adjoint); count_work
+    // is kept in every slot alike
+    wosd::BatchLaunch slot[2][2] = {{{256, 0, 64, 0}, {256, 0, 64, 0}}, {{256, 0, 64, 0}, {256, 0, 64, 0}}};
     cudaStream_t cap = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -98,6 +100,11 @@ static int upload_views(wos_batch_s *b, cudaStream_t st) {
     return 0;
 }
 
+static void set_count_work(wos_batch_s *b, int count) {
+    for (auto &d : b->slot)
+        for (auto &ph : d) ph.count_work = count;
+}
+
 // Enqueue one full step on stream st.
 static int enqueue(wos_batch_s *b, cudaStream_t st) {
     const AdjCfg a = make_adj_cfg(b->adj);
@@ -108,7 +115,7 @@ static int enqueue(wos_batch_s *b, cudaStream_t st) {
                   nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
         for (const BatchRun &r : g.runs)
             if (int rc = launch_walk_batch(g.dim, r.wl, g.d_views + r.first, g.d_cfgs + r.first, g.d_items + r.first,
-                                           r.count, r.base, r.walks, b->launch, o, g.counters, st))
+                                           r.count, r.base, r.walks, b->slot[g.dim - 2][0], o, g.counters, st))
                 return rc;
         if (int rc = launch_reduce_batch(g.vals, g.d_items, n_items, g.points, g.mean, g.var, st)) return rc;
         if (int rc = launch_loss_batch(g.mean, g.d_items, n_items, g.dLdu, g.loss, st)) return rc;
@@ -116,9 +123,38 @@ static int enqueue(wos_batch_s *b, cudaStream_t st) {
             for (const BatchRun &r : g.runs)
                 if (int rc = launch_adjoint_batch(g.dim, r.wl, g.d_views + r.first, g.d_cfgs + r.first, a,
                                                   g.d_items + r.first, r.count, r.base, r.walks, g.dLdu, g.wrec,
-                                                  g.wds, g.acc, b->launch, g.counters + 1, st))
+                                                  g.wds, g.acc, b->slot[g.dim - 2][1], g.counters + 1, st))
                     return rc;
             if (int rc = launch_acc_to_f32(g.acc, g.grad, g.acc_len, st)) return rc;
+        }
+    }
+    return 0;
+}
+
+// One phase (0 walks, 1 adjoint) of the dimension-dim group alone, over the
+// first `frac` of every run's walks (a prefix of the run's walk range), for
+// the slot tuner.  Needs a full step before it (the adjoint reads the walk
+// phase's records and dL/du); the accumulators it fills are overwritten by
+// the next full step.
+static int enqueue_slot(wos_batch_s *b, int dim, int phase, double frac, cudaStream_t st) {
+    const AdjCfg a = make_adj_cfg(b->adj);
+    for (BatchGroup &g : b->groups) {
+        if (g.dim != dim) continue;
+        WalkOut o{g.vals, nullptr, b->want_adjoint ? g.wrec : nullptr, b->want_adjoint ? g.wds : nullptr,
+                  nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+        for (const BatchRun &r : g.runs) {
+            const long long w = std::max(1LL, std::min(r.walks, (long long)(frac * (double)r.walks)));
+            if (phase == 0) {
+                if (int rc = launch_walk_batch(g.dim, r.wl, g.d_views + r.first, g.d_cfgs + r.first,
+                                               g.d_items + r.first, r.count, r.base, w, b->slot[dim - 2][0], o,
+                                               g.counters, st))
+                    return rc;
+            } else if (b->want_adjoint) {
+                if (int rc = launch_adjoint_batch(g.dim, r.wl, g.d_views + r.first, g.d_cfgs + r.first, a,
+                                                  g.d_items + r.first, r.count, r.base, w, g.dLdu, g.wrec, g.wds,
+                                                  g.acc, b->slot[dim - 2][1], g.counters + 1, st))
+                    return rc;
+            }
         }
     }
     return 0;
@@ -277,9 +313,12 @@ int wos_batch_set_launch(wos_batch_t b, int block_threads, int blocks_per_sm, in
     if (block_threads % 32 || block_threads < 32 || block_threads > 512)
         return fail(WOS_ERR_INVALID_ARGUMENT, "block_threads must be a multiple of 32 in [32, 512]");
     if (chunk < 1) return fail(WOS_ERR_INVALID_ARGUMENT, "chunk must be >= 1");
-    b->launch.block = block_threads;
-    b->launch.blocks_per_sm = std::max(0, blocks_per_sm);
-    b->launch.chunk = chunk;
+    for (auto &d : b->slot)
+        for (auto &ph : d) {
+            ph.block = block_threads;
+            ph.blocks_per_sm = std::max(0, blocks_per_sm);
+            ph.chunk = chunk;
+        }
     drop_graph(b);
     return 0;
 }
@@ -296,8 +335,9 @@ int wos_batch_autotune(wos_batch_t b, const int32_t *block_threads, const int32_
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     BT(cudaStreamIsCapturing(st, &cs));
     if (cs != cudaStreamCaptureStatusNone) return fail(WOS_ERR_INVALID_ARGUMENT, "autotune during stream capture");
-    const BatchLaunch keep = b->launch;
-    b->launch.count_work = 0;
+    BatchLaunch keep[2][2];
+    std::copy(&b->slot[0][0], &b->slot[0][0] + 4, &keep[0][0]);
+    set_count_work(b, 0);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     BT(cudaEventCreate(&e0));
     cudaError_t e = cudaEventCreate(&e1);
@@ -308,8 +348,11 @@ int wos_batch_autotune(wos_batch_t b, const int32_t *block_threads, const int32_
     int rc = 0, arg = -1;
     float best_ms = INFINITY;
     for (int i = 0; i < n_candidates && !rc; ++i) {
-        b->launch.block = block_threads[i];
-        b->launch.chunk = chunk[i];
+        for (auto &d : b->slot)
+            for (auto &ph : d) {
+                ph.block = block_threads[i];
+                ph.chunk = chunk[i];
+            }
         float t = INFINITY;
         for (int r = 0; r <= repeats && !rc; ++r) {
             if ((e = cudaEventRecord(e0, st)) != cudaSuccess) rc = fail_cuda(e, "cudaEventRecord");
@@ -328,12 +371,116 @@ int wos_batch_autotune(wos_batch_t b, const int32_t *block_threads, const int32_
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    b->launch = keep;
+    std::copy(&keep[0][0], &keep[0][0] + 4, &b->slot[0][0]);
     if (rc) return rc;
-    b->launch.block = block_threads[arg];
-    b->launch.chunk = chunk[arg];
+    for (auto &d : b->slot)
+        for (auto &ph : d) {
+            ph.block = block_threads[arg];
+            ph.chunk = chunk[arg];
+        }
     drop_graph(b);
     if (best) *best = arg;
+    return 0;
+}
+
+int wos_batch_autotune_slots(wos_batch_t b, const int32_t *block_threads, const int32_t *blocks_per_sm,
+                             const int32_t *chunk, int n_candidates, int repeats, double sample, wos_stream_t stream,
+                             float *ms, int32_t *best) {
+    if (b == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "batch is NULL");
+    if (block_threads == nullptr || blocks_per_sm == nullptr || chunk == nullptr || n_candidates < 1 ||
+        repeats < 1)
+        return fail(WOS_ERR_INVALID_ARGUMENT, "autotune needs candidates and repeats >= 1");
+    if (!(sample > 0.0 && sample <= 1.0)) return fail(WOS_ERR_INVALID_ARGUMENT, "sample must be in (0, 1]");
+    for (int i = 0; i < n_candidates; ++i)
+        if (block_threads[i] % 32 || block_threads[i] < 32 || block_threads[i] > 512 || chunk[i] < 1 ||
+            blocks_per_sm[i] < 0)
+            return fail(WOS_ERR_INVALID_ARGUMENT, "candidate " + std::to_string(i) + ": invalid launch shape");
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    BT(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return fail(WOS_ERR_INVALID_ARGUMENT, "autotune during stream capture");
+    const int count = b->slot[0][0].count_work;
+    set_count_work(b, 0);
+    for (int k = 0; k < 4; ++k) {
+        if (ms)
+            for (int i = 0; i < n_candidates; ++i) ms[k * n_candidates + i] = NAN;
+        if (best) best[k] = -1;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    BT(cudaEventCreate(&e0));
+    cudaError_t e = cudaEventCreate(&e1);
+    if (e != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail_cuda(e, "cudaEventCreate");
+    }
+    // one full step first: the adjoint slots read the walk phase's outputs
+    int rc = enqueue(b, st);
+    for (int dim = 2; dim <= 3 && !rc; ++dim) {
+        bool present = false;
+        for (const BatchGroup &g : b->groups) present = present || g.dim == dim;
+        if (!present) continue;
+        for (int phase = 0; phase < (b->want_adjoint ? 2 : 1) && !rc; ++phase) {
+            BatchLaunch &L = b->slot[dim - 2][phase];
+            const int k = (dim - 2) * 2 + phase;
+            int arg = -1;
+            float best_ms = INFINITY;
+            for (int i = 0; i < n_candidates && !rc; ++i) {
+                L.block = block_threads[i];
+                L.blocks_per_sm = blocks_per_sm[i];
+                L.chunk = chunk[i];
+                float t = INFINITY;
+                for (int r = 0; r < repeats && !rc; ++r) {
+                    if ((e = cudaEventRecord(e0, st)) != cudaSuccess) rc = fail_cuda(e, "cudaEventRecord");
+                    if (!rc) rc = enqueue_slot(b, dim, phase, sample, st);
+                    if (!rc && (e = cudaEventRecord(e1, st)) != cudaSuccess) rc = fail_cuda(e, "cudaEventRecord");
+                    if (!rc && (e = cudaEventSynchronize(e1)) != cudaSuccess) rc = fail_cuda(e, "cudaEventSynchronize");
+                    float x = 0.0f;
+                    if (!rc && (e = cudaEventElapsedTime(&x, e0, e1)) != cudaSuccess)
+                        rc = fail_cuda(e, "cudaEventElapsedTime");
+                    if (!rc) t = std::min(t, x);
+                }
+                if (ms) ms[k * n_candidates + i] = t;
+                if (!rc && t < best_ms) {
+                    best_ms = t;
+                    arg = i;
+                }
+            }
+            if (arg >= 0) {
+                L.block = block_threads[arg];
+                L.blocks_per_sm = blocks_per_sm[arg];
+                L.chunk = chunk[arg];
+            }
+            if (best) best[k] = arg;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    set_count_work(b, count);
+    drop_graph(b);
+    return rc;
+}
+
+int wos_batch_set_launch_slot(wos_batch_t b, int dim, int phase, int block_threads, int blocks_per_sm, int chunk) {
+    if (b == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "batch is NULL");
+    if (dim < 2 || dim > 3 || phase < 0 || phase > 1) return fail(WOS_ERR_INVALID_ARGUMENT, "dim 2-3, phase 0-1");
+    if (block_threads % 32 || block_threads < 32 || block_threads > 512)
+        return fail(WOS_ERR_INVALID_ARGUMENT, "block_threads must be a multiple of 32 in [32, 512]");
+    if (chunk < 1) return fail(WOS_ERR_INVALID_ARGUMENT, "chunk must be >= 1");
+    BatchLaunch &L = b->slot[dim - 2][phase];
+    L.block = block_threads;
+    L.blocks_per_sm = std::max(0, blocks_per_sm);
+    L.chunk = chunk;
+    drop_graph(b);
+    return 0;
+}
+
+int wos_batch_get_launch(wos_batch_t b, int dim, int phase, int32_t *out) {
+    if (b == nullptr || out == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "batch or out is NULL");
+    if (dim < 2 || dim > 3 || phase < 0 || phase > 1) return fail(WOS_ERR_INVALID_ARGUMENT, "dim 2-3, phase 0-1");
+    const BatchLaunch &L = b->slot[dim - 2][phase];
+    out[0] = L.block;
+    out[1] = L.blocks_per_sm;
+    out[2] = L.chunk;
     return 0;
 }
 
@@ -350,11 +497,11 @@ int wos_batch_run(wos_batch_t b, int use_graph, wos_stream_t stream) {
     // value it was captured with, so a change forces a new capture
     const int count = work_counting_enabled();
     if (!use_graph) {
-        b->launch.count_work = count;
+        set_count_work(b, count);
         return enqueue(b, st);
     }
-    if (b->exec == nullptr || b->launch.count_work != count) {
-        b->launch.count_work = count;
+    if (b->exec == nullptr || b->slot[0][0].count_work != count) {
+        set_count_work(b, count);
         if (int rc = capture(b)) return rc;
     }
     const cudaError_t e = cudaGraphLaunch(b->exec, st);

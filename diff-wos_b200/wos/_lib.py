@@ -180,6 +180,9 @@ SIGNATURES = {
                               ctypes.POINTER(_P)]),
     "wos_batch_set_launch": (_I, [_P, _I, _I, _I]),
     "wos_batch_autotune": (_I, [_P, _P, _P, _I, _I, _P, _P, _P]),
+    "wos_batch_autotune_slots": (_I, [_P, _P, _P, _P, _I, _I, ctypes.c_double, _P, _P, _P]),
+    "wos_batch_get_launch": (_I, [_P, _I, _I, _P]),
+    "wos_batch_set_launch_slot": (_I, [_P, _I, _I, _I, _I, _I]),
     "wos_batch_refresh": (_I, [_P, _P]),
     "wos_batch_run": (_I, [_P, _I, _P]),
     "wos_batch_outputs": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),

@@ -1,7 +1,8 @@
 """Launch-shape autotuner for the persistent walk / adjoint kernels.
 
 The knobs are the threads per block, the resident blocks per SM and the
-number of walks a warp takes from the global queue per grab (chunk).  Results
+number of walks a warp takes from the global queue per grab (chunk); a
+batched plan keeps one shape per (dimension, phase) slot.  Results
 never depend on them (walks are defined by their Philox counters), only speed
 does.  The tuner times a few candidates on the caller's own workload with
 CUDA events and keeps the fastest; results are cached per (GPU, dimension,
@@ -19,6 +20,11 @@ import torch
 from . import _lib
 
 CANDIDATES = [(128, 32), (256, 32), (256, 64), (256, 128), (512, 64), (128, 16)]
+# (threads per block, blocks per SM (0 = occupancy limit), walks per queue
+# grab) for the slot-wise batch tuner: block size x grab size at full
+# occupancy, plus fewer resident blocks (more L1 and shared memory per block)
+SLOT_CANDIDATES = ([(b, 0, c) for b in (128, 256, 512) for c in (16, 32, 64, 128)]
+                   + [(256, 2, 32), (256, 3, 32), (128, 4, 32), (128, 6, 32)])
 CACHE = Path(os.environ.get("WOS_B200_CACHE", Path.home() / ".cache" / "wos_b200")) / "autotune.json"
 
 
@@ -87,3 +93,11 @@ def tune_batch(plan, candidates=None, repeats: int = 1):
     """Pick the launch shape of a BatchPlan by timing whole steps (the
     library's wos_batch_autotune, on the current stream)."""
     return plan.autotune(candidates or CANDIDATES, repeats)
+
+
+def tune_batch_slots(plan, candidates=None, repeats: int = 1, sample: float = 1.0):
+    """Pick a launch shape per (dimension, phase) slot of a BatchPlan by
+    timing each slot's launches alone (wos_batch_autotune_slots): block size,
+    resident blocks per SM and walks per queue grab.  `sample` < 1 times a
+    prefix of each run's walks, for large plans."""
+    return plan.autotune_slots(candidates or SLOT_CANDIDATES, repeats, sample)

@@ -63,6 +63,39 @@ class BatchPlan:
         cands = [tuple(int(x) for x in c) for c in candidates]
         return cands[best.value], {c: float(ms[i]) for i, c in enumerate(cands)}
 
+    def autotune_slots(self, candidates, repeats: int = 1, sample: float = 1.0):
+        """Per (dimension, phase) slot, time that slot's launches alone on the
+        first `sample` fraction of its walks for each (block_threads,
+        blocks_per_sm, chunk) candidate and keep the fastest
+        (wos_batch_autotune_slots).  Returns ({slot: best candidate},
+        {slot: {candidate: ms}}) for the slots present, slot = (dim, phase)."""
+        n = len(candidates)
+        bt = (ctypes.c_int32 * n)(*[int(c[0]) for c in candidates])
+        bs = (ctypes.c_int32 * n)(*[int(c[1]) for c in candidates])
+        ch = (ctypes.c_int32 * n)(*[int(c[2]) for c in candidates])
+        ms = (ctypes.c_float * (4 * n))()
+        best = (ctypes.c_int32 * 4)()
+        call("wos_batch_autotune_slots", self.h, bt, bs, ch, n, int(repeats), float(sample), stream(), ms, best)
+        cands = [tuple(int(x) for x in c) for c in candidates]
+        chosen, times = {}, {}
+        for k in range(4):
+            if best[k] < 0:
+                continue
+            slot = (2 + k // 2, k % 2)
+            chosen[slot] = cands[best[k]]
+            times[slot] = {c: float(ms[k * n + i]) for i, c in enumerate(cands)}
+        return chosen, times
+
+    def set_launch_slot(self, dim: int, phase: int, block_threads=256, blocks_per_sm=0, chunk=64):
+        call("wos_batch_set_launch_slot", self.h, int(dim), int(phase), int(block_threads), int(blocks_per_sm),
+             int(chunk))
+
+    def launch(self, dim: int, phase: int):
+        """(block_threads, blocks_per_sm, chunk) of slot (dim, phase)."""
+        out = (ctypes.c_int32 * 3)()
+        call("wos_batch_get_launch", self.h, int(dim), int(phase), out)
+        return tuple(int(x) for x in out)
+
     def refresh(self):
         call("wos_batch_refresh", self.h, stream())
 

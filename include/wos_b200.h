@@ -415,6 +415,28 @@ WOS_API int wos_batch_set_launch(wos_batch_t b, int block_threads, int blocks_pe
 WOS_API int wos_batch_autotune(wos_batch_t b, const int32_t *block_threads, const int32_t *chunk, int n_candidates,
                                int repeats, wos_stream_t stream, float *ms, int32_t *best);
 
+/* Slot-wise launch-shape tuner: the plan keeps one launch shape per slot
+ * (dimension 2 or 3 x phase: walks, adjoint); after one full step it times,
+ * for each slot present, that slot's launches alone over the first `sample`
+ * fraction (0 < sample <= 1) of every run's walks for each candidate
+ * (block_threads[i], blocks_per_sm[i] (0 = occupancy limit), chunk[i]) --
+ * the best of `repeats` -- and keeps the fastest for that slot.  ms
+ * (4 x n_candidates floats, slot k = (dim - 2) * 2 + phase; NaN for absent
+ * slots) and best (4 indices, -1 for absent slots) may be NULL.  Results do
+ * not depend on the shapes.  Synchronises the stream; not during capture.
+ * No counterpart in the reference. */
+WOS_API int wos_batch_autotune_slots(wos_batch_t b, const int32_t *block_threads, const int32_t *blocks_per_sm,
+                                     const int32_t *chunk, int n_candidates, int repeats, double sample,
+                                     wos_stream_t stream, float *ms, int32_t *best);
+
+/* Set the launch shape of one slot (dim 2 or 3, phase 0 walks / 1 adjoint). */
+WOS_API int wos_batch_set_launch_slot(wos_batch_t b, int dim, int phase, int block_threads, int blocks_per_sm,
+                                      int chunk);
+
+/* The launch shape of slot (dim, phase 0 walks / 1 adjoint): out[0] threads
+ * per block, out[1] blocks per SM (0 = occupancy limit), out[2] chunk. */
+WOS_API int wos_batch_get_launch(wos_batch_t b, int dim, int phase, int32_t *out);
+
 /* Re-read the scenes' device views (after wos_scene_update_vertices). */
 WOS_API int wos_batch_refresh(wos_batch_t b, wos_stream_t stream);
 

@@ -76,6 +76,12 @@ def test_argument_validation_without_gpu():
     assert L.wos_batch_autotune(ctypes.c_void_p(1), bt, ch, 0, 1, None, None, None) == _lib.WOS_ERR_INVALID_ARGUMENT
     assert L.wos_batch_autotune(ctypes.c_void_p(1), bt, ch, 1, 1, None, None, None) == _lib.WOS_ERR_INVALID_ARGUMENT
     assert b"candidate 0" in L.wos_last_error_string()
+    bs = (ctypes.c_int32 * 1)(0)
+    assert L.wos_batch_autotune_slots(None, bt, bs, ch, 1, 1, 1.0, None, None, None) == _lib.WOS_ERR_INVALID_ARGUMENT
+    assert L.wos_batch_autotune_slots(ctypes.c_void_p(1), bt, bs, ch, 1, 1, 0.0, None, None, None) == \
+        _lib.WOS_ERR_INVALID_ARGUMENT
+    assert b"sample" in L.wos_last_error_string()
+    assert L.wos_batch_get_launch(ctypes.c_void_p(1), 4, 0, (ctypes.c_int32 * 3)()) == _lib.WOS_ERR_INVALID_ARGUMENT
     assert L.wos_version() >= 100
 
 

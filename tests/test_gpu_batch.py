@@ -143,3 +143,28 @@ def test_autotuned_launch_shape_does_not_change_results(cuda):
         for i in range(len(items)):
             assert np.array_equal(_np(plan.outputs(i)["mean"]), ref[i]), (bt, chunk, i)
     plan.close()
+
+
+def test_slot_tuner_picks_shapes_per_dimension_and_phase(cuda):
+    """wos_batch_autotune_slots keeps one launch shape per (dimension, phase)
+    slot present in the plan; results stay bit-identical whatever it picks
+    (also when it timed only a prefix of each run's walks)."""
+    from wos import BatchPlan, autotune
+    from wos.native import AdjointSettings
+    items, _ = _batched_items(3, 2, 0.01, seed=8)
+    adj = AdjointSettings(epsilon2=1e-3, clamping=0.1, want_dV=True, want_dg=True, want_dsrc=False)
+    plan = BatchPlan(items, adj)
+    plan.run(use_graph=False)
+    ref = [(_np(plan.outputs(i)["mean"]), _np(plan.outputs(i)["dg"])) for i in range(len(items))]
+    cands = [(128, 0, 16), (256, 2, 32), (512, 0, 64)]
+    chosen, times = autotune.tune_batch_slots(plan, candidates=cands, repeats=1, sample=0.5)
+    assert set(chosen) == {(2, 0), (2, 1), (3, 0), (3, 1)}
+    for slot, c in chosen.items():
+        assert c in cands and plan.launch(*slot) == c
+        assert len(times[slot]) == 3 and all(np.isfinite(v) and v > 0 for v in times[slot].values())
+    plan.run(use_graph=True)
+    for i in range(len(items)):
+        m, dg = ref[i]
+        assert np.array_equal(_np(plan.outputs(i)["mean"]), m), i
+        np.testing.assert_allclose(_np(plan.outputs(i)["dg"]), dg, rtol=1e-5, atol=1e-7 * np.abs(dg).max())
+    plan.close()
