@@ -76,10 +76,10 @@ def test_vertex_gradients_match_fd_within_standard_errors(cuda):
     from wos.native import NativeScene
     V, F, g, P = _setup(nseg=512, grid=64)
     rng = np.random.default_rng(1)
-    ks = rng.choice(len(V), 16, replace=False)
-    dirs = rng.normal(size=(16, 2))
+    ks = rng.choice(len(V), 24, replace=False)
+    dirs = rng.normal(size=(24, 2))
     dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
-    seeds = list(range(100, 112))
+    seeds = list(range(100, 116))
     h = 1e-3
     adj = np.zeros((len(seeds), len(ks)))
     fd = np.zeros((len(seeds), len(ks)))
@@ -95,6 +95,8 @@ def test_vertex_gradients_match_fd_within_standard_errors(cuda):
             fd[si, j] = (_loss(Vp, F, g, SRC, P, seed, 256) - _loss(Vm, F, g, SRC, P, seed, 256)) / (2 * h)
     se = np.sqrt(adj.var(0, ddof=1) / len(seeds) + fd.var(0, ddof=1) / len(seeds))
     z = (adj.mean(0) - fd.mean(0)) / np.maximum(se, 1e-12)
-    # within 2 standard errors for the large majority; none wildly off
-    assert np.mean(np.abs(z) < 2.0) >= 0.8, z
-    assert np.all(np.abs(z) < 4.0), z
+    # epsilon (1e-3) is well below the segment length (~1.3e-2), where the
+    # finite difference of the shell-terminated estimator and the adjoint's
+    # boundary-shape derivative agree (h = 1e-3, the configured step)
+    assert np.mean(np.abs(z) < 2.0) >= 0.9, z
+    assert np.all(np.abs(z) < 3.0), z
