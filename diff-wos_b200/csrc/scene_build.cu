@@ -406,93 +406,181 @@ __global__ void k_leaf_data(const unsigned long long *keys, int n, const float4 
     }
 }
 
-// Wide-tree leaves.  Leaf i holds Morton positions [WT_LEAF i, WT_LEAF i +
-// WT_LEAF): its box, and its slab bound -- n = the normalised sum of the
-// primitives' unit normals, c = the box centre computed exactly as the query
-// does, and [oc - oh, oc + oh] covering n.(v - c) over the primitives'
-// vertices as the distance code sees them (a and a + d for a segment, a,
-// a + ab, a + ac for a triangle), evaluated in double and widened by the
-// float roundings plus a relative margin.  A leaf whose normals cancel gets
-// n = 0 and oh = inf (no slab bound).
+// Wide-tree leaf boxes.  Leaf i holds sorted positions [WT_LEAF i, WT_LEAF i
+// + WT_LEAF); its box is the union of its primitives' boxes and bounds it in
+// the level above.
 template <int D>
-__global__ void k_wt_level1(const unsigned long long *keys, int nF, const float *pbox, const float4 *lseg,
-                            const float4 *ltri, float4 *out, float4 *slab, int n1) {
+__global__ void k_wt_level1(const unsigned long long *keys, int nF, const float *pbox, float4 *out, int n1) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n1) return;
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     const int b0 = WT_LEAF * i, e = min(b0 + WT_LEAF, nF);
-    double ns[3] = {0.0, 0.0, 0.0};
     for (int s = b0; s < e; ++s) {
         const float *b = pbox + (size_t)(unsigned)keys[s] * 2 * D;
         for (int k = 0; k < D; ++k) {
             lo[k] = fminf(lo[k], b[k]);
             hi[k] = fmaxf(hi[k], b[D + k]);
         }
-        double nn[3] = {0.0, 0.0, 0.0};
-        if (D == 2) {
-            const float4 g = lseg[s];
-            nn[0] = (double)g.w;
-            nn[1] = -(double)g.z;
-        } else {
-            const float4 ab = ltri[3 * s + 1], ac = ltri[3 * s + 2];
-            nn[0] = (double)ab.y * ac.z - (double)ab.z * ac.y;
-            nn[1] = (double)ab.z * ac.x - (double)ab.x * ac.z;
-            nn[2] = (double)ab.x * ac.y - (double)ab.y * ac.x;
-        }
-        const double l = sqrt(nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2]);
-        if (l > 0.0)
-            for (int k = 0; k < 3; ++k) ns[k] += nn[k] / l;
-    }
-    float c[3] = {0.0f, 0.0f, 0.0f};
-    for (int k = 0; k < D; ++k) c[k] = (lo[k] + hi[k]) * 0.5f;
-    const double ln = sqrt(ns[0] * ns[0] + ns[1] * ns[1] + ns[2] * ns[2]);
-    float nf[3] = {0.0f, 0.0f, 0.0f};
-    float ocf = 0.0f, ohf = INFINITY;
-    if (ln > 1e-6) {
-        // unit normal, shrunk by 2^-20 so that |n| <= 1 after rounding
-        for (int k = 0; k < D; ++k) nf[k] = (float)(ns[k] / ln * (1.0 - 0x1p-20));
-        double omin = INFINITY, omax = -INFINITY, diag2 = 0.0;
-        for (int k = 0; k < D; ++k) diag2 += ((double)hi[k] - lo[k]) * ((double)hi[k] - lo[k]);
-        for (int s = b0; s < e; ++s) {
-            double v[3][3];
-            int nv;
-            if (D == 2) {
-                const float4 g = lseg[s];
-                v[0][0] = g.x;
-                v[0][1] = g.y;
-                v[1][0] = (double)g.x + g.z;
-                v[1][1] = (double)g.y + g.w;
-                v[0][2] = v[1][2] = 0.0;
-                nv = 2;
-            } else {
-                const float4 a = ltri[3 * s], ab = ltri[3 * s + 1], ac = ltri[3 * s + 2];
-                const double av[3] = {a.x, a.y, a.z}, abv[3] = {ab.x, ab.y, ab.z}, acv[3] = {ac.x, ac.y, ac.z};
-                for (int k = 0; k < 3; ++k) {
-                    v[0][k] = av[k];
-                    v[1][k] = av[k] + abv[k];
-                    v[2][k] = av[k] + acv[k];
-                }
-                nv = 3;
-            }
-            for (int j = 0; j < nv; ++j) {
-                double o = 0.0;
-                for (int k = 0; k < D; ++k) o += (double)nf[k] * (v[j][k] - (double)c[k]);
-                omin = fmin(omin, o);
-                omax = fmax(omax, o);
-            }
-        }
-        const double oc = 0.5 * (omin + omax);
-        ocf = (float)oc;
-        const double oh = 0.5 * (omax - omin) + fabs(oc - (double)ocf) + 1e-6 * sqrt(diag2);
-        ohf = __double2float_ru(oh);
     }
     if (D == 2) {
         out[i] = make_float4(lo[0], lo[1], hi[0], hi[1]);
-        slab[i] = make_float4(nf[0], nf[1], ocf, ohf);
     } else {
-        out[2 * i] = make_float4(lo[0], lo[1], lo[2], ohf);
+        out[2 * i] = make_float4(lo[0], lo[1], lo[2], 0.0f);
         out[2 * i + 1] = make_float4(hi[0], hi[1], hi[2], 0.0f);
-        slab[i] = make_float4(nf[0], nf[1], nf[2], ocf);
+    }
+}
+
+// Eigenvectors of a symmetric 3 x 3 matrix by cyclic Jacobi rotations in
+// double: on return the columns of v are orthonormal and a is (nearly)
+// diagonal, a[k][k] the eigenvalue of column k.
+__device__ void sym3_eigen(double a[3][3], double v[3][3]) {
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) v[r][c] = r == c ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 32; ++sweep) {
+        const double off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
+        const double dia = a[0][0] * a[0][0] + a[1][1] * a[1][1] + a[2][2] * a[2][2];
+        if (!(off > 1e-30 * dia)) break;
+        for (int p = 0; p < 2; ++p) {
+            for (int q = p + 1; q < 3; ++q) {
+                if (a[p][q] == 0.0) continue;
+                // rotation in the (p, q) plane that zeroes a[p][q]: A <- J^T A J
+                const double th = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
+                const double t = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                for (int k = 0; k < 3; ++k) {
+                    const double akp = a[k][p], akq = a[k][q];
+                    a[k][p] = c * akp - s * akq;
+                    a[k][q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    const double apk = a[p][k], aqk = a[q][k];
+                    a[p][k] = c * apk - s * aqk;
+                    a[q][k] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    const double vkp = v[k][p], vkq = v[k][q];
+                    v[k][p] = c * vkp - s * vkq;
+                    v[k][q] = s * vkp + c * vkq;
+                }
+            }
+        }
+    }
+}
+
+// Oriented box of each wide-tree leaf, the bound the queries test leaves by.
+// Its axes are the principal axes of the leaf's vertices as the distance code
+// sees them (a and a + d for a segment; a, a + ab, a + ac for a triangle):
+// the eigenvectors of their covariance, rounded to float and shrunk by 2^-20
+// so that the float axes, with the third 3D axis u2 = u0 x u1 evaluated in
+// float exactly as the query does (cross3), form a matrix of norm below 1.
+// The centre c is rounded to float, and e_k bounds |u_k.(y - c)| over the
+// vertices y, evaluated in double with the float axes and centre and widened
+// by 1e-6 |y - c|max, which covers the query's float rounding of q - c and of
+// the dot products (relative 2^-22 of |q - c| <= |q - y| + |y - c|).  Layout:
+// 2D (u0.x, u0.y, c.x, c.y), (e0, e1, 0, 0) with u1 = (-u0.y, u0.x); 3D
+// (u0, e0), (u1, e1), (c, e2).
+template <int D>
+__global__ void k_wt_obb(const float4 *lseg, const float4 *ltri, int nF, float4 *obb, int n1) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n1) return;
+    const int b0 = WT_LEAF * i, e = min(b0 + WT_LEAF, nF);
+    constexpr int NV = D == 2 ? 2 : 3;
+    auto vertex = [&](int s, int j, double *y) {
+        if (D == 2) {
+            const float4 g = lseg[s];
+            y[0] = j == 0 ? (double)g.x : (double)g.x + g.z;
+            y[1] = j == 0 ? (double)g.y : (double)g.y + g.w;
+            y[2] = 0.0;
+        } else {
+            const float4 a = ltri[3 * s], ab = ltri[3 * s + 1], ac = ltri[3 * s + 2];
+            y[0] = j == 0 ? (double)a.x : (double)a.x + (j == 1 ? ab.x : ac.x);
+            y[1] = j == 0 ? (double)a.y : (double)a.y + (j == 1 ? ab.y : ac.y);
+            y[2] = j == 0 ? (double)a.z : (double)a.z + (j == 1 ? ab.z : ac.z);
+        }
+    };
+    double m[3] = {0.0, 0.0, 0.0}, y[3];
+    for (int s = b0; s < e; ++s)
+        for (int j = 0; j < NV; ++j) {
+            vertex(s, j, y);
+            for (int k = 0; k < D; ++k) m[k] += y[k];
+        }
+    const double nv = (double)((e - b0) * NV);
+    for (int k = 0; k < D; ++k) m[k] /= nv;
+    double cov[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    for (int s = b0; s < e; ++s)
+        for (int j = 0; j < NV; ++j) {
+            vertex(s, j, y);
+            for (int r = 0; r < D; ++r)
+                for (int c = 0; c < D; ++c) cov[r][c] += (y[r] - m[r]) * (y[c] - m[c]);
+        }
+    // float axes u[k][*]
+    float u[3][3] = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
+    const double shrink = 1.0 - 0x1p-20;
+    if (D == 2) {
+        const double th = 0.5 * atan2(2.0 * cov[0][1], cov[0][0] - cov[1][1]);
+        u[0][0] = (float)(cos(th) * shrink);
+        u[0][1] = (float)(sin(th) * shrink);
+        u[1][0] = -u[0][1];
+        u[1][1] = u[0][0];
+    } else {
+        double vec[3][3];
+        sym3_eigen(cov, vec);
+        // u0, u1: the two largest-variance axes; u2 = u0 x u1 (the normal)
+        int o[3] = {0, 1, 2};
+        for (int a = 0; a < 2; ++a)
+            for (int b = a + 1; b < 3; ++b)
+                if (cov[o[b]][o[b]] > cov[o[a]][o[a]]) {
+                    const int t = o[a];
+                    o[a] = o[b];
+                    o[b] = t;
+                }
+        for (int k = 0; k < 3; ++k) {
+            u[0][k] = (float)(vec[k][o[0]] * shrink);
+            u[1][k] = (float)(vec[k][o[1]] * shrink);
+        }
+        cross3(u[0][0], u[0][1], u[0][2], u[1][0], u[1][1], u[1][2], u[2][0], u[2][1], u[2][2]);
+    }
+    // centre: the middle of the projection ranges about the mean
+    double pmin[3] = {INFINITY, INFINITY, INFINITY}, pmax[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int s = b0; s < e; ++s)
+        for (int j = 0; j < NV; ++j) {
+            vertex(s, j, y);
+            for (int k = 0; k < D; ++k) {
+                double p = 0.0;
+                for (int c = 0; c < D; ++c) p += (double)u[k][c] * (y[c] - m[c]);
+                pmin[k] = fmin(pmin[k], p);
+                pmax[k] = fmax(pmax[k], p);
+            }
+        }
+    float cf[3] = {0.0f, 0.0f, 0.0f};
+    for (int c = 0; c < D; ++c) {
+        double x = m[c];
+        for (int k = 0; k < D; ++k) x += 0.5 * (pmin[k] + pmax[k]) * (double)u[k][c];
+        cf[c] = (float)x;
+    }
+    double ext[3] = {0.0, 0.0, 0.0}, r2 = 0.0;
+    for (int s = b0; s < e; ++s)
+        for (int j = 0; j < NV; ++j) {
+            vertex(s, j, y);
+            double d2 = 0.0;
+            for (int c = 0; c < D; ++c) d2 += (y[c] - cf[c]) * (y[c] - cf[c]);
+            r2 = fmax(r2, d2);
+            for (int k = 0; k < D; ++k) {
+                double p = 0.0;
+                for (int c = 0; c < D; ++c) p += (double)u[k][c] * (y[c] - (double)cf[c]);
+                ext[k] = fmax(ext[k], fabs(p));
+            }
+        }
+    const double pad = 1e-6 * sqrt(r2);
+    float ef[3];
+    for (int k = 0; k < D; ++k) ef[k] = __double2float_ru(ext[k] + pad);
+    if (D == 2) {
+        obb[2 * i] = make_float4(u[0][0], u[0][1], cf[0], cf[1]);
+        obb[2 * i + 1] = make_float4(ef[0], ef[1], 0.0f, 0.0f);
+    } else {
+        obb[3 * i] = make_float4(u[0][0], u[0][1], u[0][2], ef[0]);
+        obb[3 * i + 1] = make_float4(u[1][0], u[1][1], u[1][2], ef[1]);
+        obb[3 * i + 2] = make_float4(cf[0], cf[1], cf[2], ef[2]);
     }
 }
 
@@ -528,9 +616,11 @@ __global__ void k_wt_level(const float4 *in, int n_in, float4 *out, int n_out) {
 }
 
 // Slab bounds of the level-2 nodes of a 3D wide tree (patches of up to 1024
-// triangles), the same construction as the leaves' in k_wt_level1: the
-// normalised sum of the unit face normals, and the interval of n.(v - c) over
-// the vertices, c the node's box centre, widened for rounding.  One block of
+// triangles): n = the normalised sum of the unit face normals, and the
+// interval [oc - oh, oc + oh] of n.(v - c) over the vertices v as the distance
+// code sees them, c the node's box centre computed exactly as the query does,
+// evaluated in double and widened by the float roundings plus a relative
+// margin.  A node whose normals cancel gets n = 0 and oh = inf (no slab).  One block of
 // SLAB_THREADS per node; fixed-order reductions.  The half-thickness goes to
 // the box's first .w, the normal and the interval's centre to slab[node].
 constexpr int SLAB_THREADS = 256;
@@ -618,7 +708,7 @@ static cudaError_t dalloc(T **p, size_t count, cudaStream_t st) {
 }
 
 void SceneImpl::release(cudaStream_t st) {
-    void *ptrs[] = {V, F, N, g, seg, seginv, tri, node, lseg, lseginv, ltri, lorig, cdf, wt_box, wt_slab, guide};
+    void *ptrs[] = {V, F, N, g, seg, seginv, tri, node, lseg, lseginv, ltri, lorig, cdf, wt_box, wt_slab, wt_obb, guide};
     for (void *p : ptrs)
         if (p) cudaFreeAsync(p, st);
     V = nullptr;
@@ -636,6 +726,7 @@ void SceneImpl::release(cudaStream_t st) {
     cdf = nullptr;
     wt_box = nullptr;
     wt_slab = nullptr;
+    wt_obb = nullptr;
     guide = nullptr;
 }
 
@@ -788,17 +879,20 @@ static int build_geometry(SceneImpl &S, cudaStream_t st) {
         WOS_TRY(dalloc(&S.wt_box, (size_t)off * W, st));
         if (S.wt_slab) cudaFreeAsync(S.wt_slab, st);
         S.wt_slab = nullptr;
-        const bool slab2 = D == 3 && WOS_SLAB_LEVELS >= 2 && S.wt_levels >= 2;
-        WOS_TRY(dalloc(&S.wt_slab, (size_t)S.wt_count[1] + (slab2 ? S.wt_count[2] : 0), st));
-        k_wt_level1<D><<<nblk(S.wt_count[1], TB), TB, 0, st>>>(skeys, nF, pbox, S.lseg, S.ltri, S.wt_box, S.wt_slab,
-                                                               S.wt_count[1]);
+        if (S.wt_obb) cudaFreeAsync(S.wt_obb, st);
+        S.wt_obb = nullptr;
+        const bool slab2 = D == 3 && S.wt_levels >= 2;
+        WOS_TRY(dalloc(&S.wt_slab, slab2 ? (size_t)S.wt_count[2] : 0, st));
+        WOS_TRY(dalloc(&S.wt_obb, (size_t)S.wt_count[1] * (D == 2 ? 2 : 3), st));
+        k_wt_level1<D><<<nblk(S.wt_count[1], TB), TB, 0, st>>>(skeys, nF, pbox, S.wt_box, S.wt_count[1]);
+        k_wt_obb<D><<<nblk(S.wt_count[1], 64), 64, 0, st>>>(S.lseg, S.ltri, nF, S.wt_obb, S.wt_count[1]);
         for (int l = 2; l <= S.wt_levels; ++l)
             k_wt_level<D><<<nblk(S.wt_count[l], TB), TB, 0, st>>>(S.wt_box + (size_t)S.wt_off[l - 1] * W,
                                                                 S.wt_count[l - 1], S.wt_box + (size_t)S.wt_off[l] * W,
                                                                 S.wt_count[l]);
         if (slab2)
             k_wt_slab2<<<S.wt_count[2], SLAB_THREADS, 0, st>>>(S.ltri, nF, S.wt_box + (size_t)S.wt_off[2] * W,
-                                                               S.wt_slab + S.wt_count[1], S.wt_count[2]);
+                                                               S.wt_slab, S.wt_count[2]);
         WOS_TRY(cudaGetLastError());
     }
 
@@ -951,6 +1045,7 @@ SceneView SceneImpl::view() const {
     }
     v.wt_box = wt_box;
     v.wt_slab = wt_slab;
+    v.wt_obb = wt_obb;
     return v;
 }
 

@@ -55,6 +55,7 @@ struct SceneImpl {
     int wt_off[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     float4 *wt_box = nullptr;
     float4 *wt_slab = nullptr;
+    float4 *wt_obb = nullptr;
 
     int allocate(cudaStream_t st);
     int check_indices(cudaStream_t st);

@@ -68,19 +68,22 @@ struct SceneView {
     // primitives [WT_LEAF i, WT_LEAF i + WT_LEAF) (in Morton order); level k
     // node i bounds level k-1 nodes [32 i, 32 i + 32); level wt_levels has at
     // most 32 nodes.  Boxes: 2D one float4 (lo.x, lo.y, hi.x, hi.y) per node,
-    // 3D two float4 (lo.xyz, w), (hi.xyz, 0) with w = 0 except at leaves; level
-    // k starts at wt_box[wt_off[k]] (in nodes).  Each leaf also has a slab
-    // bound: unit normal n and [oc - oh, oc + oh] containing n.(v - c) for
-    // every vertex v of its primitives, c the box centre; 2D wt_slab[i] =
-    // (n.x, n.y, oc, oh), 3D wt_slab[i] = (n.xyz, oc) with oh in the leaf
-    // box's lo.w.  Any point y of the leaf is at least |n.(x - c) - oc| - oh
-    // from x, which for flat patches tilted against the axes is far tighter
-    // than the box.
+    // 3D two float4 (lo.xyz, w), (hi.xyz, 0); level k starts at
+    // wt_box[wt_off[k]] (in nodes).  The queries bound a leaf by its oriented
+    // box instead (wt_obb, built by k_wt_obb): principal axes u_k of its
+    // vertices, a centre c and half-extents e_k with |u_k.(y - c)| <= e_k;
+    // 2D two float4 (u0.xy, c.xy), (e0, e1, 0, 0) with u1 = (-u0.y, u0.x), 3D
+    // three (u0, e0), (u1, e1), (c, e2) with u2 = u0 x u1.  A 3D level-2 node
+    // also has a slab bound: unit normal n and [oc - oh, oc + oh] containing
+    // n.(v - c) for every vertex v, c its box centre; wt_slab[i] = (n.xyz, oc)
+    // with oh in the box's lo.w.  Any point y of the node is at least
+    // |n.(x - c) - oc| - oh from x.
     int wt_levels;
     int wt_count[8];
     int wt_off[8];
     const float4 *wt_box;
     const float4 *wt_slab;
+    const float4 *wt_obb;
 };
 
 constexpr int WT_MAX_LEVELS = 5;
@@ -516,27 +519,52 @@ __device__ __forceinline__ float wt_box_d2(const SceneView &S, int node, const f
     return box_d2<D>(lo, hi, q);
 }
 
-// 3D levels whose nodes carry a slab bound beside their box: the leaves and,
-// with WOS_SLAB_LEVELS 2, their parents (patches of 1024 triangles, whose box
-// is loose wherever the surface is tilted against the axes).
-#ifndef WOS_SLAB_LEVELS
-#define WOS_SLAB_LEVELS 2
-#endif
+// Lower bound on the squared distance from q to leaf `leaf`: the distance to
+// its oriented box, sum_k max(|u_k.(q - c)| - e_k, 0)^2, scaled by
+// (1 - 2^-18).  With |u_k.(y - c)| <= e_k for every point y of the leaf and
+// the axes' matrix of norm below 1, the exact value is at most |q - y|^2; the
+// float roundings of q - c and of the dot products (relative 2^-22 of
+// |q - c|) are covered by the 1e-6 |y - c| margin in e_k for the |y - c| part
+// and by the final scale for the rest, so the result stays below |q - y|^2 --
+// a bound as safe as the box distance, and tighter wherever a leaf's patch or
+// arc is tilted against the axes.
+template <int D>
+__device__ __forceinline__ float leaf_obb_d2(const SceneView &S, int leaf, const float *q) {
+    constexpr float SHRINK = 0.999996185302734375f;  // 1 - 2^-18
+    if (D == 2) {
+        const float4 a = __ldg(&S.wt_obb[2 * leaf]), e = __ldg(&S.wt_obb[2 * leaf + 1]);
+        const float vx = q[0] - a.z, vy = q[1] - a.w;
+        const float a0 = fmaxf(fabsf(dot2(a.x, a.y, vx, vy)) - e.x, 0.0f);
+        const float a1 = fmaxf(fabsf(dot2(-a.y, a.x, vx, vy)) - e.y, 0.0f);
+        return fmaf(a0, a0, a1 * a1) * SHRINK;
+    }
+    const float4 f0 = __ldg(&S.wt_obb[3 * leaf]), f1 = __ldg(&S.wt_obb[3 * leaf + 1]),
+                 f2 = __ldg(&S.wt_obb[3 * leaf + 2]);
+    float u2[3];
+    cross3(f0.x, f0.y, f0.z, f1.x, f1.y, f1.z, u2[0], u2[1], u2[2]);
+    const float vx = q[0] - f2.x, vy = q[1] - f2.y, vz = q[2] - f2.z;
+    const float a0 = fmaxf(fabsf(dot3(f0.x, f0.y, f0.z, vx, vy, vz)) - f0.w, 0.0f);
+    const float a1 = fmaxf(fabsf(dot3(f1.x, f1.y, f1.z, vx, vy, vz)) - f1.w, 0.0f);
+    const float a2 = fmaxf(fabsf(dot3(u2[0], u2[1], u2[2], vx, vy, vz)) - f2.w, 0.0f);
+    return fmaf(a0, a0, fmaf(a1, a1, a2 * a2)) * SHRINK;
+}
 
-// Lower bound on the squared distance from q to node `node` of level L: in 3D
-// (levels up to WOS_SLAB_LEVELS) the larger of its box distance and its slab
-// distance; otherwise, and in 2D, the box distance (polyline pieces are thin
-// enough in their boxes that the slab test costs more than it prunes).  The
-// slabs of level 2 follow those of level 1 in wt_slab.
+// Lower bound on the squared distance from q to node `node` of level L: a
+// leaf's oriented-box distance; for a 3D level-2 node (a patch of 1024
+// triangles, whose box is loose wherever the surface is tilted against the
+// axes) the larger of its box distance and its slab distance; otherwise the
+// box distance.
 template <int D, int L>
 __device__ __forceinline__ float node_bound(const SceneView &S, int node, const float *q) {
     float lo[3], hi[3], n[3], c[3], oc, oh;
-    if (D == 2 || L > WOS_SLAB_LEVELS) {
+    if constexpr (L == 1) {
+        return leaf_obb_d2<D>(S, node, q);
+    } else if (D == 2 || L > 2) {
         return wt_box_d2<D>(S, S.wt_off[L] + node, q);
     } else {
         const int bi = S.wt_off[L] + node;
         const float4 a = __ldg(&S.wt_box[2 * bi]), b = __ldg(&S.wt_box[2 * bi + 1]);
-        const float4 sl = __ldg(&S.wt_slab[L == 1 ? node : S.wt_count[1] + node]);
+        const float4 sl = __ldg(&S.wt_slab[node]);
         lo[0] = a.x;
         lo[1] = a.y;
         lo[2] = a.z;
