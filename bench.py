@@ -949,7 +949,8 @@ def main():
     fused_ws = torch.empty(_lib.lib().wos_solve_adjoint_workspace_size(scene.h, n, ctypes.byref(c), ctypes.byref(ca)),
                            dtype=torch.uint8, device=dev)
     solve_ws = torch.empty(_lib.lib().wos_solve_workspace_size(n, ctypes.byref(c)), dtype=torch.uint8, device=dev)
-    adj_ws = torch.empty(_lib.lib().wos_adjoint_workspace_size(scene.h), dtype=torch.uint8, device=dev)
+    adj_ws = torch.empty(_lib.lib().wos_adjoint_records_workspace_size(scene.h, n, ctypes.byref(c)),
+                         dtype=torch.uint8, device=dev)
 
     def step(seed):
         """One fused forward + adjoint step (wos_solve_adjoint, loss = mean(u^2))."""

@@ -51,6 +51,12 @@ struct BatchGroup {
     double *acc = nullptr;
     float *grad = nullptr;  // float copy of acc
     unsigned long long *counters = nullptr;
+    // adjoint sample order (launch_batch_order): sort keys, workspace, and
+    // the sorted indices of the last enqueued step (inside order_ws)
+    long long nkeys = 0;
+    void *order_ws = nullptr;
+    size_t order_bytes = 0;
+    const unsigned *order = nullptr;
 };
 
 }  // namespace wosd
@@ -78,8 +84,8 @@ namespace wosd {
     } while (0)
 
 static void free_group(BatchGroup &g, cudaStream_t st) {
-    void *ptrs[] = {g.d_items, g.d_views, g.d_cfgs, g.vals, g.wrec, g.wds, g.mean, g.var, g.loss,
-                    g.dLdu,    g.acc,     g.grad,   g.counters};
+    void *ptrs[] = {g.d_items, g.d_views, g.d_cfgs, g.vals, g.wrec,     g.wds,     g.mean,
+                    g.var,     g.loss,    g.dLdu,   g.acc,  g.grad, g.counters, g.order_ws};
     for (void *p : ptrs)
         if (p) cudaFreeAsync(p, st);
 }
@@ -120,10 +126,13 @@ static int enqueue(wos_batch_s *b, cudaStream_t st) {
         if (int rc = launch_reduce_batch(g.vals, g.d_items, n_items, g.points, g.mean, g.var, st)) return rc;
         if (int rc = launch_loss_batch(g.mean, g.d_items, n_items, g.dLdu, g.loss, st)) return rc;
         if (b->want_adjoint) {
+            if (int rc = launch_batch_order(g.dim, g.d_views, g.d_items, n_items, g.nkeys, g.wrec, g.walks,
+                                            g.order_ws, g.order_bytes, &g.order, st))
+                return rc;
             for (const BatchRun &r : g.runs)
                 if (int rc = launch_adjoint_batch(g.dim, r.wl, g.d_views + r.first, g.d_cfgs + r.first, a,
                                                   g.d_items + r.first, r.count, r.base, r.walks, g.dLdu, g.wrec,
-                                                  g.wds, g.acc, b->slot[g.dim - 2][1], g.counters + 1, st))
+                                                  g.wds, g.acc, b->slot[g.dim - 2][1], g.counters + 1, g.order, st))
                     return rc;
             if (int rc = launch_acc_to_f32(g.acc, g.grad, g.acc_len, st)) return rc;
         }
@@ -152,7 +161,7 @@ static int enqueue_slot(wos_batch_s *b, int dim, int phase, double frac, cudaStr
             } else if (b->want_adjoint) {
                 if (int rc = launch_adjoint_batch(g.dim, r.wl, g.d_views + r.first, g.d_cfgs + r.first, a,
                                                   g.d_items + r.first, r.count, r.base, w, g.dLdu, g.wrec, g.wds,
-                                                  g.acc, b->slot[dim - 2][1], g.counters + 1, st))
+                                                  g.acc, b->slot[dim - 2][1], g.counters + 1, g.order, st))
                     return rc;
             }
         }
@@ -234,6 +243,8 @@ int wos_batch_create(const wos_batch_item *items, int n_items, const wos_adjoint
         g.acc_len += S.nV;
         d.ds_off = g.acc_len;
         g.acc_len += 5;
+        d.prim_off = g.nkeys;
+        g.nkeys += (long long)S.nF + 1;
         const int wl = specialised_depth(S.wt_levels);
         if (g.runs.empty() || g.runs.back().wl != wl) {
             BatchRun r;
@@ -282,6 +293,8 @@ int wos_batch_create(const wos_batch_item *items, int n_items, const wos_adjoint
             if (g.has_src && b->adj.want_dsrc) A(&g.wds, sizeof(float) * 5 * W);
             A(&g.acc, sizeof(double) * g.acc_len);
             A(&g.grad, sizeof(float) * g.acc_len);
+            g.order_bytes = batch_order_bytes(g.nkeys, g.walks);
+            if (g.order_bytes) A(&g.order_ws, g.order_bytes);
         }
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(g.d_items, g.items.data(), sizeof(BatchItemDev) * NI, cudaMemcpyHostToDevice, st);

@@ -461,6 +461,7 @@ size_t wos_solve_adjoint_workspace_size(wos_scene_t scene, int n, const wos_para
     if (wants_wds(S, *p, *a)) b += align256(sizeof(float) * 5 * nw);  // per-walk source derivatives
     b += align256(sizeof(float) * (size_t)n);                         // dL/du
     b += adj_acc(S, nullptr).bytes;                                   // gradient accumulators
+    b += align256(record_order_bytes(S.nF, (long long)nw));           // sample order
     return b;
 }
 
@@ -509,6 +510,7 @@ int wos_solve_adjoint(wos_scene_t scene, const float *P, int n, const wos_params
     const AdjAcc acc = adj_acc(S, b);
     cudaError_t e = cudaMemsetAsync(b, 0, acc.bytes, st);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(adjoint accumulators)");
+    b += acc.bytes;
     WalkOut o{vals, nullptr, wrec, wds, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     if (int rc = launch_walk(S, P, (long long)nw, *p, false, o, counter, st)) return rc;
     if (int rc = launch_reduce(vals, n, p->nwalks, mean, var, st)) return rc;
@@ -519,6 +521,8 @@ int wos_solve_adjoint(wos_scene_t scene, const float *P, int n, const wos_params
     ao.dsrc = acc.ds;
     ao.wrec = wrec;
     ao.wds = wds;
+    if (int rc = launch_record_order(S, wrec, (long long)nw, b, need - (size_t)(b - s.base), &ao.order, st))
+        return rc;
     if (int rc = launch_adjoint(S, P, (long long)nw, *p, make_adj(*a), dLdu, ADJ_FROM_RECORDS, ao, counter, st))
         return rc;
     return finish_adjoint(S, a, acc, dV, dg, dsrc, st);
@@ -533,6 +537,7 @@ size_t wos_solve_tangent_workspace_size(wos_scene_t scene, int n, const wos_para
     b += align256(wos_walk_record_bytes(S.dim) * nw);                 // per-walk records
     if (wants_wds(S, *p, *a)) b += align256(sizeof(float) * 5 * nw);  // per-walk source derivatives
     b += align256(sizeof(float) * nw);                                // per-walk tangents
+    b += align256(record_order_bytes(S.nF, (long long)nw));           // sample order
     return b;
 }
 
@@ -572,6 +577,7 @@ int wos_solve_tangent(wos_scene_t scene, const float *P, int n, const wos_params
         b += align256(sizeof(float) * 5 * nw);
     }
     float *tan = (float *)b;
+    b += align256(sizeof(float) * nw);
     cudaError_t e = cudaMemsetAsync(tan, 0, sizeof(float) * nw, st);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(tangents)");
     WalkOut o{vals, nullptr, wrec, wds, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -584,6 +590,8 @@ int wos_solve_tangent(wos_scene_t scene, const float *P, int n, const wos_params
     ao.tg = dg_dir;
     ao.ts = dsrc_dir;
     ao.tan = tan;
+    if (int rc = launch_record_order(S, wrec, (long long)nw, b, need - (size_t)(b - s.base), &ao.order, st))
+        return rc;
     if (int rc = launch_adjoint(S, P, (long long)nw, *p, make_adj(*a), nullptr, ADJ_TANGENT, ao, counter, st))
         return rc;
     return launch_reduce(tan, n, p->nwalks, tangent, tangent_var, st);
@@ -716,6 +724,12 @@ int wos_solve_records(wos_scene_t scene, const float *P, int n, const wos_params
     return launch_reduce(vals, n, p->nwalks, mean, var, st);
 }
 
+size_t wos_adjoint_records_workspace_size(wos_scene_t scene, int n, const wos_params *p) {
+    if (scene == nullptr || p == nullptr || n < 0 || p->nwalks < 1) return 0;
+    return wos_adjoint_workspace_size(scene) +
+           align256(record_order_bytes(scene->impl.nF, (long long)n * (long long)p->nwalks));
+}
+
 int wos_adjoint_records(wos_scene_t scene, const float *P, int n, const wos_params *p, const wos_adjoint_params *a,
                         const float *dLdu, const void *records, const float *dcontrib, float *dV, float *dg,
                         float *dsrc, void *workspace, size_t workspace_bytes, wos_stream_t stream) {
@@ -739,8 +753,10 @@ int wos_adjoint_records(wos_scene_t scene, const float *P, int n, const wos_para
     WOS_CHECK_DEV_OPT(dsrc, "dsrc");
     cudaStream_t st = (cudaStream_t)stream;
     const size_t need = wos_adjoint_workspace_size(scene);
+    const size_t need_ordered = wos_adjoint_records_workspace_size(scene, n, p);
+    const bool ordered = workspace == nullptr || workspace_bytes >= need_ordered;
     Scratch s;
-    if (int rc = s.init(workspace, workspace_bytes, need, st)) return rc;
+    if (int rc = s.init(workspace, workspace_bytes, ordered ? need_ordered : need, st)) return rc;
     unsigned long long *counter = (unsigned long long *)s.base;
     const AdjAcc acc = adj_acc(S, s.base + 256);
     cudaError_t e = cudaMemsetAsync(s.base, 0, need, st);
@@ -751,6 +767,10 @@ int wos_adjoint_records(wos_scene_t scene, const float *P, int n, const wos_para
     ao.dsrc = acc.ds;
     ao.wrec = (const int *)records;
     ao.wds = dcontrib;
+    if (ordered && need_ordered > need)
+        if (int rc = launch_record_order(S, ao.wrec, (long long)n * p->nwalks, s.base + need, need_ordered - need,
+                                         &ao.order, st))
+            return rc;
     if (int rc = launch_adjoint(S, P, (long long)n * p->nwalks, *p, make_adj(*a), dLdu, ADJ_FROM_RECORDS, ao, counter,
                                 st))
         return rc;
@@ -758,6 +778,8 @@ int wos_adjoint_records(wos_scene_t scene, const float *P, int n, const wos_para
 }
 
 int wos_set_work_counting(int enable) { return set_work_counting(enable); }
+
+int wos_set_sample_order(int mode) { return set_sample_order(mode); }
 
 int wos_work_counters(int reset, int64_t *out) {
     if (out == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "out is NULL");

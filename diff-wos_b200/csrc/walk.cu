@@ -18,6 +18,9 @@
 // tangent_derivative (wos/scene.py:451-460, wos/wos3d.py:137-156), OursCUDA /
 // Ours3D (wos/wos_grad.py:130-151, wos/wos_grad_3d.py:117-137).
 #include <algorithm>
+#include <climits>
+
+#include <cub/cub.cuh>
 
 #include "scene_impl.h"
 #include "walk.h"
@@ -79,7 +82,13 @@ __device__ __forceinline__ void flush_work(const Work &wk) {
 // ball of radius ball_m centred at x (wball): it gets that primitive, or
 // prim = -1 when none blocks.  Brute force runs per lane and always returns
 // the nearest primitive.  Must be called by all 32 lanes.
-template <int D, bool BVH, int WL = 0>
+//
+// SAME: a lane whose query point is bit for bit the one the warp answered
+// just before takes that answer.  The nearest primitive does not depend on
+// the warm candidate, so this changes no result; in the forward kernels the
+// lanes that start walks of one point in the same iteration ask the same first
+// query -- the one farthest from the boundary and the most expensive.
+template <int D, bool BVH, int WL = 0, bool SAME = false>
 __device__ __forceinline__ Hit warp_queries(const SceneView &S, bool active, const float *x, int warm, Work &work,
                                             float ball_m = -1.0f) {
     Hit mine{-1, INFINITY};
@@ -90,6 +99,9 @@ __device__ __forceinline__ Hit warp_queries(const SceneView &S, bool active, con
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     unsigned act = __ballot_sync(FULL, active);
+    unsigned prev[3] = {0u, 0u, 0u};
+    bool have = false;
+    Hit h{-1, INFINITY};
     while (act) {
         const int j = __ffs(act) - 1;
         act &= act - 1u;
@@ -99,7 +111,19 @@ __device__ __forceinline__ Hit warp_queries(const SceneView &S, bool active, con
         q[2] = D == 3 ? __shfl_sync(FULL, x[2], j) : 0.0f;
         const int wp = __shfl_sync(FULL, warm, j);
         const float bm = __shfl_sync(FULL, ball_m, j);
-        Hit h{-1, INFINITY};
+        if (SAME) {
+            const bool same = have && __float_as_uint(q[0]) == prev[0] && __float_as_uint(q[1]) == prev[1] &&
+                              (D == 2 || __float_as_uint(q[2]) == prev[2]);
+            prev[0] = __float_as_uint(q[0]);
+            prev[1] = __float_as_uint(q[1]);
+            prev[2] = __float_as_uint(q[2]);
+            have = true;
+            if (same) {
+                if (lane == j) mine = h;
+                continue;
+            }
+        }
+        h = Hit{-1, INFINITY};
         if (bm > 0.0f) {
             wball<D, WL>(S, q, bm, h, work);
         } else {
@@ -299,7 +323,7 @@ __global__ void __launch_bounds__(512) k_walk(SceneView S, WalkCfg c, const floa
             walk_origin<D>(c, P, pt, wk, x0);
             w.start(x0, D);
         }
-        const Hit hit = warp_queries<D, BVH, WL>(S, active, w.p, w.last, work);
+        const Hit hit = warp_queries<D, BVH, WL, true>(S, active, w.p, w.last, work);
         if (!active) continue;
         w.last = hit.prim;
         const int r = walker_advance<D>(w, S, hit, c, c.eps, c.project != 0, c.prevent_fd != 0, pt, wk, ROLE_PRIMAL,
@@ -815,6 +839,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, Wa
                 }
                 phase = PH_ND_START;
             } else {
+                if (FROM_REC && out.order != nullptr) idx = (long long)__ldg(&out.order[idx]);
                 pt = (uint32_t)(idx / c.nwalks);
                 wk = c.walk_offset + (uint32_t)(idx - (long long)pt * c.nwalks);
                 W = TAN ? 1.0 : (double)__ldg(&dLdu[pt]) / c.nwalks;
@@ -1853,6 +1878,90 @@ int launch_adjoint(const SceneImpl &S, const float *P, long long total, const wo
 #undef WOS_ADJ
 }
 
+// ------------------------------------------------------------------ sample order
+// Adjoint samples that start from forward records run in the order of their
+// boundary primitive along the trees' primitive order (curve order in 2D,
+// Hilbert order in 3D).  Every sample begins with the inscribed-ball
+// bisection and the first steps of its ball walks next to that primitive, so
+// in this order the lanes of a warp -- and the warps the GPU runs at the same
+// time -- query the same leaves, which then stay in L1.  Results do not depend
+// on the order: each sample draws from its own Philox counters; only the
+// summation order of the FP64 gradient atomics changes.
+static int g_sample_order = 1;
+
+int set_sample_order(int mode) {
+    g_sample_order = mode ? 1 : 0;
+    return 0;
+}
+
+int sample_order_mode() { return g_sample_order; }
+
+__global__ void k_prim_rank(const int *__restrict__ lorig, int nF, unsigned *rank) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nF) rank[__ldg(&lorig[s])] = (unsigned)s;
+}
+
+template <int D>
+__global__ void k_record_keys(const int *__restrict__ wrec, long long total, const unsigned *__restrict__ rank, int nF,
+                              unsigned *keys, unsigned *ids) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += stride) {
+        const int code = __ldg(&wrec[i * walkrec_words(D)]);
+        const int prim = code & 0x3fffffff;
+        keys[i] = (code < 0 || prim >= nF) ? (unsigned)nF : __ldg(&rank[prim]);
+        ids[i] = (unsigned)i;
+    }
+}
+
+// Bits of a radix-sort key whose largest value is n.
+static int key_bits_ll(long long n) {
+    int b = 1;
+    while (b < 32 && (1LL << b) <= n) ++b;
+    return b;
+}
+static int key_bits(int nF) { return key_bits_ll(nF); }
+
+size_t record_order_bytes(int nF, long long total) {
+    if (!g_sample_order || total <= 1 || total > (long long)INT_MAX || nF <= 0) return 0;
+    cub::DoubleBuffer<unsigned> k(nullptr, nullptr), v(nullptr, nullptr);
+    size_t tmp = 0;
+    if (cub::DeviceRadixSort::SortPairs(nullptr, tmp, k, v, (int)total, 0, key_bits(nF)) != cudaSuccess) return 0;
+    const auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    return al(sizeof(unsigned) * (size_t)nF) + 4 * al(sizeof(unsigned) * (size_t)total) + al(tmp);
+}
+
+int launch_record_order(const SceneImpl &S, const int *wrec, long long total, void *ws, size_t ws_bytes,
+                        const unsigned **order, cudaStream_t st) {
+    *order = nullptr;
+    const size_t need = record_order_bytes(S.nF, total);
+    if (need == 0) return 0;
+    if (ws == nullptr || ws_bytes < need) return fail(WOS_ERR_WORKSPACE, "record order: workspace too small");
+    const auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    char *b = (char *)ws;
+    unsigned *rank = (unsigned *)b;
+    b += al(sizeof(unsigned) * (size_t)S.nF);
+    unsigned *buf[4];
+    for (int i = 0; i < 4; ++i) {
+        buf[i] = (unsigned *)b;
+        b += al(sizeof(unsigned) * (size_t)total);
+    }
+    const size_t tmp_bytes = need - (size_t)(b - (char *)ws);
+    k_prim_rank<<<(S.nF + 255) / 256, 256, 0, st>>>(S.lorig, S.nF, rank);
+    const int G = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    if (S.dim == 2)
+        k_record_keys<2><<<G, 256, 0, st>>>(wrec, total, rank, S.nF, buf[0], buf[2]);
+    else
+        k_record_keys<3><<<G, 256, 0, st>>>(wrec, total, rank, S.nF, buf[0], buf[2]);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_record_keys launch");
+    cub::DoubleBuffer<unsigned> k(buf[0], buf[1]), v(buf[2], buf[3]);
+    size_t tmp = tmp_bytes;
+    e = cub::DeviceRadixSort::SortPairs(b, tmp, k, v, (int)total, 0, key_bits(S.nF), st);
+    if (e != cudaSuccess) return fail_cuda(e, "record order sort");
+    *order = v.Current();
+    return 0;
+}
+
 int launch_add_f64(const double *src, float *dst, long long n, cudaStream_t st) {
     if (n == 0 || dst == nullptr) return 0;
     const int B = 256;
@@ -1894,13 +2003,17 @@ __device__ __forceinline__ int find_item_point(const BatchItemDev *__restrict__ 
     return lo;
 }
 
-template <int D, int WL = 0>
+// SAME: as in warp_queries (same item and point: the previous answer).
+template <int D, int WL = 0, bool SAME = false>
 __device__ __forceinline__ Hit warp_queries_batch(const SceneView *__restrict__ views, bool active, int item,
                                                   const float *x, int warm, Work &work, float ball_m = -1.0f) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     Hit mine{-1, INFINITY};
     unsigned act = __ballot_sync(FULL, active);
+    unsigned prev[3] = {0u, 0u, 0u};
+    int prev_it = -1;
+    Hit h{-1, INFINITY};
     while (act) {
         const int j = __ffs(act) - 1;
         act &= act - 1u;
@@ -1911,8 +2024,20 @@ __device__ __forceinline__ Hit warp_queries_batch(const SceneView *__restrict__ 
         const int wp = __shfl_sync(FULL, warm, j);
         const int it = __shfl_sync(FULL, item, j);
         const float bm = __shfl_sync(FULL, ball_m, j);
+        if (SAME) {
+            const bool same = it == prev_it && __float_as_uint(q[0]) == prev[0] &&
+                              __float_as_uint(q[1]) == prev[1] && (D == 2 || __float_as_uint(q[2]) == prev[2]);
+            prev[0] = __float_as_uint(q[0]);
+            prev[1] = __float_as_uint(q[1]);
+            prev[2] = __float_as_uint(q[2]);
+            prev_it = it;
+            if (same) {
+                if (lane == j) mine = h;
+                continue;
+            }
+        }
         const SceneView &Sj = views[it];
-        Hit h{-1, INFINITY};
+        h = Hit{-1, INFINITY};
         if (bm > 0.0f) {
             wball<D, WL>(Sj, q, bm, h, work);
         } else {
@@ -1957,7 +2082,7 @@ __global__ void __launch_bounds__(512) k_walk_batch(const SceneView *__restrict_
             walk_origin<D>(cfgs[item], it.P, pt, wk, x0);
             w.start(x0, D);
         }
-        const Hit hit = warp_queries_batch<D, WL>(views, active, item, w.p, w.last, work);
+        const Hit hit = warp_queries_batch<D, WL, true>(views, active, item, w.p, w.last, work);
         if (!active) continue;
         const SceneView &S = views[item];
         const WalkCfg &c = cfgs[item];
@@ -2055,7 +2180,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
     const BatchItemDev *__restrict__ items, int n_items, long long base, long long total,
     const float *__restrict__ dLdu,
     unsigned long long *counter, int chunk, const int *__restrict__ wrec, const float *__restrict__ wds, double *acc,
-    int count_work) {
+    int count_work, const unsigned *__restrict__ order) {
     extern __shared__ float4 smem[];
     // source-gradient accumulators only when the launch has source derivatives
     // (the launcher sizes shared memory the same way)
@@ -2092,6 +2217,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
         if (!refill(q, active, idx, counter, total, chunk)) break;
         if (active && !was) {
             idx += base;
+            if (order != nullptr) idx = (long long)__ldg(&order[idx]);
             item = find_item(items, n_items, idx);
             const BatchItemDev &it = items[item];
             const SceneView &S = views[item];
@@ -2318,28 +2444,123 @@ template <int D, int WL>
 static int launch_adjoint_batch_t(const SceneView *views, const WalkCfg *cfgs, const AdjCfg &a,
                                   const BatchItemDev *items, int n_items, long long base, long long total,
                                   const float *dLdu, const int *wrec, const float *wds, double *acc,
-                                  const BatchLaunch &L, unsigned long long *counter, cudaStream_t st) {
+                                  const BatchLaunch &L, unsigned long long *counter, const unsigned *order,
+                                  cudaStream_t st) {
     const int block = std::min(L.block, 256);
     const size_t smem = (size_t)block * adj_thread_bytes<D>(wds != nullptr) + 16;
     const int chunk = std::max(1, L.chunk / 2);
     int grid = 0;
     if (int rc = persistent_grid(k_adjoint_batch<D, WL>, block, smem, L.blocks_per_sm, grid)) return rc;
     k_adjoint_batch<D, WL><<<grid, block, smem, st>>>(views, cfgs, a, items, n_items, base, total, dLdu, counter,
-                                                      chunk, wrec, wds, acc, L.count_work);
+                                                      chunk, wrec, wds, acc, L.count_work, order);
+    return 0;
+}
+
+// Sample order of a batch group's adjoint (the batched counterpart of
+// launch_record_order): keys are item-major -- item i owns the key range
+// [prim_off_i, prim_off_i + nF_i], its invalid records taking the last key --
+// so the sorted order keeps every item's samples, and so every run's, in
+// their own walk range, each sorted by boundary primitive.
+__device__ __forceinline__ int find_item_prim(const BatchItemDev *__restrict__ items, int n_items, long long s) {
+    int lo = 0, hi = n_items - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&items[mid].prim_off) <= s)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void k_batch_prim_rank(const SceneView *__restrict__ views, const BatchItemDev *__restrict__ items,
+                                  int n_items, long long nprims, unsigned *rank) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nprims; s += stride) {
+        const int i = find_item_prim(items, n_items, s);
+        const long long off = __ldg(&items[i].prim_off);
+        const long long local = s - off;
+        if (local < views[i].nF) rank[off + __ldg(&views[i].lorig[local])] = (unsigned)s;
+    }
+}
+
+template <int D>
+__global__ void k_batch_record_keys(const SceneView *__restrict__ views, const BatchItemDev *__restrict__ items,
+                                    int n_items, const int *__restrict__ wrec, long long total,
+                                    const unsigned *__restrict__ rank, unsigned *keys, unsigned *ids) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += stride) {
+        const int it = find_item(items, n_items, i);
+        const long long off = __ldg(&items[it].prim_off);
+        const int nF = views[it].nF;
+        const int code = __ldg(&wrec[i * walkrec_words(D)]);
+        const int prim = code & 0x3fffffff;
+        keys[i] = (code < 0 || prim >= nF) ? (unsigned)(off + nF) : __ldg(&rank[off + prim]);
+        ids[i] = (unsigned)i;
+    }
+}
+
+static size_t batch_order_bytes_any_mode(long long nkeys, long long total) {
+    if (total <= 1 || total > (long long)INT_MAX || nkeys <= 0 || nkeys > (long long)UINT_MAX) return 0;
+    cub::DoubleBuffer<unsigned> k(nullptr, nullptr), v(nullptr, nullptr);
+    size_t tmp = 0;
+    if (cub::DeviceRadixSort::SortPairs(nullptr, tmp, k, v, (int)total, 0, key_bits_ll(nkeys)) != cudaSuccess)
+        return 0;
+    const auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    return al(sizeof(unsigned) * (size_t)nkeys) + 4 * al(sizeof(unsigned) * (size_t)total) + al(tmp);
+}
+
+size_t batch_order_bytes(long long nkeys, long long total) {
+    return g_sample_order ? batch_order_bytes_any_mode(nkeys, total) : 0;
+}
+
+// A plan sized for an order (created in mode 1) keeps it.
+int launch_batch_order(int D, const SceneView *views, const BatchItemDev *items, int n_items, long long nkeys,
+                       const int *wrec, long long total, void *ws, size_t ws_bytes, const unsigned **order,
+                       cudaStream_t st) {
+    *order = nullptr;
+    if (ws == nullptr || ws_bytes == 0 || total <= 1) return 0;
+    const size_t need = batch_order_bytes_any_mode(nkeys, total);
+    if (need == 0) return 0;
+    if (ws_bytes < need) return fail(WOS_ERR_WORKSPACE, "batch order: workspace too small");
+    const auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    char *b = (char *)ws;
+    unsigned *rank = (unsigned *)b;
+    b += al(sizeof(unsigned) * (size_t)nkeys);
+    unsigned *buf[4];
+    for (int i = 0; i < 4; ++i) {
+        buf[i] = (unsigned *)b;
+        b += al(sizeof(unsigned) * (size_t)total);
+    }
+    const size_t tmp_bytes = need - (size_t)(b - (char *)ws);
+    const int GP = (int)std::min<long long>((nkeys + 255) / 256, 148 * 16);
+    k_batch_prim_rank<<<GP, 256, 0, st>>>(views, items, n_items, nkeys, rank);
+    const int G = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    if (D == 2)
+        k_batch_record_keys<2><<<G, 256, 0, st>>>(views, items, n_items, wrec, total, rank, buf[0], buf[2]);
+    else
+        k_batch_record_keys<3><<<G, 256, 0, st>>>(views, items, n_items, wrec, total, rank, buf[0], buf[2]);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e, "k_batch_record_keys launch");
+    cub::DoubleBuffer<unsigned> k(buf[0], buf[1]), v(buf[2], buf[3]);
+    size_t tmp = tmp_bytes;
+    e = cub::DeviceRadixSort::SortPairs(b, tmp, k, v, (int)total, 0, key_bits_ll(nkeys), st);
+    if (e != cudaSuccess) return fail_cuda(e, "batch order sort");
+    *order = v.Current();
     return 0;
 }
 
 int launch_adjoint_batch(int D, int wl, const SceneView *views, const WalkCfg *cfgs, const AdjCfg &a,
                          const BatchItemDev *items, int n_items, long long base, long long total,
                          const float *dLdu, const int *wrec, const float *wds, double *acc, const BatchLaunch &L,
-                         unsigned long long *counter, cudaStream_t st) {
+                         unsigned long long *counter, const unsigned *order, cudaStream_t st) {
     if (total == 0 || n_items == 0) return 0;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counter)");
     int rc = 0;
 #define WOS_AB(DD, WW)                                                                                        \
     rc = launch_adjoint_batch_t<DD, WW>(views, cfgs, a, items, n_items, base, total, dLdu, wrec, wds, acc, L, \
-                                        counter, st)
+                                        counter, order, st)
     if (D == 2) {
         if (wl == 1) WOS_AB(2, 1); else if (wl == 2) WOS_AB(2, 2); else if (wl == 3) WOS_AB(2, 3); else WOS_AB(2, 0);
     } else {

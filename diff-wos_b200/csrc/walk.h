@@ -60,6 +60,9 @@ struct AdjOut {
     // parameters (5), each may be null; per-walk directional derivative out
     const float *tV, *tg, *ts;
     float *tan;
+    // records and tangent modes: sample processed at queue position i, or
+    // null for queue order (launch_record_order)
+    const unsigned *order;
 };
 
 // ADJ_TANGENT: forward mode from records -- each walk's derivative along a
@@ -76,6 +79,7 @@ struct BatchItemDev {
     int loss_kind;           // 0: dL/du given, 1: mean(u^2), 2: mean((u - target)^2)
     const float *target;     // n floats (kinds 0 and 2)
     long long dV_off, dg_off, ds_off;  // offsets of its FP64 gradient accumulators
+    long long prim_off;      // first sort key of its primitives (sum of nF + 1 over earlier items)
 };
 
 struct BatchLaunch {
@@ -99,7 +103,13 @@ int launch_walk_batch(int D, int wl, const SceneView *views, const WalkCfg *cfgs
 int launch_adjoint_batch(int D, int wl, const SceneView *views, const WalkCfg *cfgs, const AdjCfg &a,
                          const BatchItemDev *items, int n_items, long long base, long long total,
                          const float *dLdu, const int *wrec, const float *wds, double *acc, const BatchLaunch &L,
-                         unsigned long long *counter, cudaStream_t st);
+                         unsigned long long *counter, const unsigned *order, cudaStream_t st);
+// Sample order of a batch group's adjoint (see launch_record_order): nkeys =
+// sum of nF + 1 over the group's items; 0 bytes: no order for this size.
+size_t batch_order_bytes(long long nkeys, long long total);
+int launch_batch_order(int D, const SceneView *views, const BatchItemDev *items, int n_items, long long nkeys,
+                       const int *wrec, long long total, void *ws, size_t ws_bytes, const unsigned **order,
+                       cudaStream_t st);
 int launch_reduce_batch(const float *vals, const BatchItemDev *items, int n_items, int n_points, double *mean,
                         double *var, cudaStream_t st);
 int launch_loss_batch(const double *mean, const BatchItemDev *items, int n_items, float *dLdu, double *loss,
@@ -127,6 +137,18 @@ int launch_ball(const SceneImpl &S, const uint8_t *valid, const float *pt, const
                 bool bvh, float *R, cudaStream_t st);
 int launch_adjoint(const SceneImpl &S, const float *P, long long total, const wos_params &p, const AdjCfg &a,
                    const float *dLdu, int mode, const AdjOut &out, unsigned long long *counter, cudaStream_t st);
+// Processing order of adjoint samples that start from forward records: the
+// sample indices [0, total) sorted by the position of their record's boundary
+// primitive in the trees' primitive order (invalid records last).  Workspace
+// bytes for `total` samples on a scene of nF primitives (0: no order for
+// this size), and the launch writing the order into that workspace; *order
+// receives the sorted indices (inside the workspace).
+size_t record_order_bytes(int nF, long long total);
+int launch_record_order(const SceneImpl &S, const int *wrec, long long total, void *ws, size_t ws_bytes,
+                        const unsigned **order, cudaStream_t st);
+// 1 (default): adjoint samples from records run in record order; 0: queue order.
+int set_sample_order(int mode);
+int sample_order_mode();
 int launch_loss(const double *mean, int n, int kind, const float *target_or_dLdu, float *dLdu, double *loss,
                 cudaStream_t st);
 int launch_add_f64(const double *src, float *dst, long long n, cudaStream_t st);

@@ -8,7 +8,8 @@ CUDA tensors and every compute path runs in libwos_b200.so through its C ABI
 """
 from . import _lib, shapes
 from .batch import BatchItem, BatchPlan
-from ._lib import WosError, device_status, get_launch_config, set_launch_config, set_work_counting, work_counters
+from ._lib import (WosError, device_status, get_launch_config, set_launch_config, set_sample_order,
+                   set_work_counting, work_counters)
 from .scene import BoundarySamplingRecord, ClosestPointRecord, Detector, Intersection, Polyline
 from .scene3d import ClosestPointRecord3D, Detector3D, Detector3DY, Scene3D
 from .solver import ControlVarianceType, CustomSolver, Sampler, Solver
@@ -25,6 +26,7 @@ __all__ = [
     "BoundarySamplingRecord", "ClosestPointRecord", "ClosestPointRecord3D", "ControlVarianceType", "CustomSolver",
     "Detector", "Detector3D", "Detector3DY", "Intersection", "Ours", "Ours3D", "OursCUDA", "Polyline", "Sampler",
     "Scene3D", "Solver", "Statistics", "WoS", "WoS3D", "WoS3DCUDA", "WoSCUDA", "WoSWithSource", "WoSWithSourceCUDA",
-    "Baseline", "WosError", "device_status", "get_launch_config", "set_launch_config", "set_work_counting",
+    "Baseline", "WosError", "device_status", "get_launch_config", "set_launch_config", "set_sample_order",
+    "set_work_counting",
     "work_counters", "shapes", "BatchItem", "BatchPlan", "WoSBoundary", "Baseline2", "Baseline2CUDA", "Baseline23D", "Baseline3D",
 ]

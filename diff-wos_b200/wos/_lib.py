@@ -148,6 +148,7 @@ SIGNATURES = {
         [_P, _P, _P, _P, _P, _P, _P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams), _P, _P],
     ),
     "wos_adjoint_workspace_size": (_S, [_P]),
+    "wos_adjoint_records_workspace_size": (_S, [_P, _I, ctypes.POINTER(WosParams)]),
     "wos_adjoint": (
         _I,
         [_P, _P, _I, ctypes.POINTER(WosParams), ctypes.POINTER(WosAdjointParams), _P, _P, _P, _P, _P, _S, _P],
@@ -191,6 +192,7 @@ SIGNATURES = {
                             ctypes.POINTER(ctypes.c_int32)]),
     "wos_batch_destroy": (_I, [_P, _P]),
     "wos_set_work_counting": (_I, [_I]),
+    "wos_set_sample_order": (_I, [_I]),
     "wos_work_counters": (_I, [_I, ctypes.POINTER(ctypes.c_int64)]),
     "wos_set_launch_config": (_I, [_I, ctypes.POINTER(WosLaunchConfig)]),
     "wos_get_launch_config": (_I, [_I, ctypes.POINTER(WosLaunchConfig)]),
@@ -232,6 +234,11 @@ def device_status(reset: bool = False) -> int:
 
 def set_work_counting(enable: bool) -> None:
     call("wos_set_work_counting", int(enable))
+
+
+def set_sample_order(mode: int) -> None:
+    """1: adjoint samples from records run sorted by boundary primitive; 0: in queue order."""
+    call("wos_set_sample_order", int(mode))
 
 
 def work_counters(reset: bool = False) -> dict:

@@ -265,7 +265,7 @@ class NativeScene:
         ds = torch.zeros(5, dtype=torch.float32, device=d) if a.want_dsrc else None
         if n:
             c, ca = s.c(), a.c()
-            need = _lib.lib().wos_adjoint_workspace_size(self.h)
+            need = _lib.lib().wos_adjoint_records_workspace_size(self.h, n, ctypes.byref(c))
             if workspace is None or workspace.numel() < need:
                 workspace = torch.empty(need, dtype=torch.uint8, device=d)
             call("wos_adjoint_records", self.h, P.data_ptr(), n, ctypes.byref(c), ctypes.byref(ca), dLdu.data_ptr(),

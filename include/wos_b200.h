@@ -263,7 +263,10 @@ WOS_API int wos_solve_records(wos_scene_t scene, const float *P, int n, const wo
  * wos_solve_records (same P, n and params) instead of walking it again --
  * the reference recomputes the primal walk from the seed
  * (wos/solver.py:109-114); the records make that recomputation unnecessary
- * and the result is the same. */
+ * and the result is the same.  Its workspace is wos_adjoint_workspace_size
+ * bytes; given wos_adjoint_records_workspace_size bytes (or NULL) it also runs
+ * the samples in boundary-primitive order (wos_set_sample_order). */
+WOS_API size_t wos_adjoint_records_workspace_size(wos_scene_t scene, int n, const wos_params *p);
 WOS_API int wos_adjoint_records(wos_scene_t scene, const float *P, int n, const wos_params *p,
                                 const wos_adjoint_params *a, const float *dLdu, const void *records,
                                 const float *dcontrib, float *dV, float *dg, float *dsrc, void *workspace,
@@ -500,6 +503,17 @@ typedef struct wos_launch_config {
  * wos_work_counters reads it (synchronising the device); reset != 0 clears. */
 WOS_API int wos_set_work_counting(int enable);
 WOS_API int wos_work_counters(int reset, int64_t *out);
+
+/* Order in which the adjoint kernel runs the samples of wos_solve_adjoint and
+ * wos_solve_tangent.  mode 1 (default): sorted by the position of each walk's
+ * boundary primitive in the scene's primitive order (one radix sort of the
+ * walk records per call), so samples that start next to each other run
+ * together and share the tree's cached leaves; mode 0: in (point, walk)
+ * order.  Results are the same in both modes up to the summation order of
+ * the FP64 gradient sums.  The mode changes the workspace size: query the
+ * *_workspace_size functions after setting it.  No counterpart in the
+ * reference (one thread per walk, in launch order). */
+WOS_API int wos_set_sample_order(int mode);
 
 WOS_API int wos_set_launch_config(int dim, const wos_launch_config *cfg);
 WOS_API int wos_get_launch_config(int dim, wos_launch_config *out);
