@@ -1058,7 +1058,7 @@ def main():
         "adjoint_pts_per_s": world * n * args.steps / t_max,
         "breakdown_ms": {"forward_kernel_and_reduce": float(np.mean(t_solve)) * 1e3, "adjoint": adj_avg * 1e3,
                          "note": "separate calls of the fused step's kernels"},
-        "gpu_launches": args.steps * 7,
+        "gpu_launches": args.steps * fused_step_launches(len(F)),
         "device_status": status,
         "plain_vs_persistent": plain,
         "walk_steps": steps_stats,
@@ -1118,6 +1118,18 @@ def main():
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def fused_step_launches(nF: int) -> int:
+    """This library's kernel launches in one fused wos_solve_adjoint step
+    (dV, dg and dsrc wanted, sample order on): k_walk, k_reduce, k_loss,
+    k_prim_rank, k_record_keys, the radix sort's histogram and prefix-sum
+    kernels plus one onesweep pass per 8 key bits (keys up to nF), k_adjoint,
+    and three k_add_f64_to_f32."""
+    bits = 1
+    while bits < 32 and (1 << bits) <= nF:
+        bits += 1
+    return 9 + 2 + (bits + 7) // 8
 
 
 def fp64_accuracy(scene, V, F, g, P, P_d, threads, npts=256, ref_walks=16384):
