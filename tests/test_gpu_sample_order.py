@@ -105,3 +105,27 @@ def test_batch_sample_order_leaves_results_unchanged(cuda):
             if o0.get(k) is not None:
                 _close(o1[k], o0[k])
     assert wos.device_status() == 0
+
+
+def test_records_adjoint_with_minimal_workspace_runs_unsorted(cuda):
+    """wos_adjoint_records given only wos_adjoint_workspace_size bytes runs the
+    samples in queue order instead of failing, with the same gradients."""
+    import ctypes
+    import torch
+    from wos import _lib
+    ns, P, s, a = _case("sphere")
+    mean, _, rec, dc = ns.solve_records(P, s)
+    dLdu = (2.0 / len(P)) * mean.float()
+    ref = ns.adjoint_records(P, s, a, dLdu, rec, dc)
+    c, ca = s.c(), a.c()
+    small = _lib.lib().wos_adjoint_workspace_size(ns.h)
+    full = _lib.lib().wos_adjoint_records_workspace_size(ns.h, len(P), ctypes.byref(c))
+    assert full > small
+    ws = torch.empty(small, dtype=torch.uint8, device="cuda")
+    dV = torch.zeros((ns.nV, 3), dtype=torch.float32, device="cuda")
+    dg = torch.zeros(ns.nV, dtype=torch.float32, device="cuda")
+    _lib.call("wos_adjoint_records", ns.h, P.data_ptr(), len(P), ctypes.byref(c), ctypes.byref(ca), dLdu.data_ptr(),
+              rec.data_ptr(), None, dV.data_ptr(), dg.data_ptr(), None, ws.data_ptr(), small,
+              torch.cuda.current_stream().cuda_stream)
+    _close(dV, ref[0])
+    _close(dg, ref[1])
