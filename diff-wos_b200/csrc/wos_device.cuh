@@ -298,6 +298,16 @@ struct Work {
     unsigned nq, nb, np;
 };
 
+// The same interface counting nothing: the query functions take either type,
+// and the hot kernels run with NoWork unless work accounting is switched on
+// (the counters' registers and adds cost 1-3 % of a step).
+struct NoCount {
+    __device__ __forceinline__ NoCount &operator+=(unsigned) { return *this; }
+};
+struct NoWork {
+    NoCount nq, nb, np;
+};
+
 // Pruning slack (same rule as the oracle): a box is skipped only when its
 // squared distance exceeds (1 + 2^-10) best + 1025 (s 2^-20)^2, where s
 // bounds the coordinates' magnitude around the scene.
@@ -313,8 +323,8 @@ __device__ __forceinline__ float prune_bound(float best, float tol2) { return fm
 
 // Brute-force nearest over the original primitive order, ties to the lowest
 // index (include/scene.cuh:102-128).
-template <int D>
-__device__ __forceinline__ Hit nearest_brute(const SceneView &S, const float *p, Work &wk) {
+template <int D, class WK>
+__device__ __forceinline__ Hit nearest_brute(const SceneView &S, const float *p, WK &wk) {
     Hit h{-1, INFINITY};
     wk.nq += 1;
     wk.np += (unsigned)S.nF;
@@ -389,9 +399,9 @@ __device__ __forceinline__ void load_node(const float4 *base, int k, float (*lo)
 // LBVH nearest: nearest-first descent with a per-thread stack, conservative
 // pruning, ties to the lowest original index.  The first n_top nodes (the
 // shallowest, breadth-first) are read from shared memory.
-template <int D>
+template <int D, class WK>
 __device__ __forceinline__ Hit nearest_bvh(const SceneView &S, const float *p, const float4 *top, int n_top,
-                                           int *status, Work &wk) {
+                                           int *status, WK &wk) {
     Hit h{-1, INFINITY};
     wk.nq += 1;
     if (S.nF == 1) {
@@ -620,9 +630,9 @@ __device__ __forceinline__ float wt_bound(float best, float tol2) { return fminf
 // warm-start candidate (a real primitive with its distance); pruning is
 // conservative, so the result is the exact minimum of (d2, primitive index)
 // -- the same as the brute-force search.
-template <int D, int L>
+template <int D, int L, class WK>
 __device__ __forceinline__ void wdescend(const SceneView &S, const float *q, int first, float tol2, Hit &best,
-                                         Work &wk) {
+                                         WK &wk) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int child = first + lane;
@@ -663,8 +673,8 @@ __device__ __forceinline__ void wdescend(const SceneView &S, const float *q, int
 
 // WL > 0: the tree has exactly WL levels (a kernel compiled for one depth
 // holds one descent, which keeps its code small); WL = 0: any depth.
-template <int D, int WL = 0>
-__device__ __forceinline__ Hit wquery(const SceneView &S, const float *q, Hit best, Work &wk) {
+template <int D, int WL = 0, class WK>
+__device__ __forceinline__ Hit wquery(const SceneView &S, const float *q, Hit best, WK &wk) {
     const float tol2 = prune_tol2<D>(S, q);
     wk.nq += 1;
     if constexpr (WL > 0) {
@@ -692,9 +702,9 @@ __device__ __forceinline__ Hit wquery(const SceneView &S, const float *q, Hit be
 // blocking primitive.
 __device__ __forceinline__ bool ball_blocks(float d2, float m) { return sqrtf(d2) - m < -1e-5f; }
 
-template <int D, int L>
+template <int D, int L, class WK>
 __device__ __forceinline__ bool wball_descend(const SceneView &S, const float *q, int first, float bound, float m,
-                                              Hit &hit, Work &wk) {
+                                              Hit &hit, WK &wk) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int child = first + lane;
@@ -733,8 +743,8 @@ __device__ __forceinline__ bool wball_descend(const SceneView &S, const float *q
 // at q: returns true with a blocking primitive in `hit`, or false when no
 // primitive blocks.  Boxes are pruned against m^2 with the nearest search's
 // conservative tolerance, so no blocking primitive is missed.
-template <int D, int WL = 0>
-__device__ __forceinline__ bool wball(const SceneView &S, const float *q, float m, Hit &hit, Work &wk) {
+template <int D, int WL = 0, class WK>
+__device__ __forceinline__ bool wball(const SceneView &S, const float *q, float m, Hit &hit, WK &wk) {
     const float bound = wt_bound((m * m) * (1.0f + 0x1p-20f), prune_tol2<D>(S, q));
     wk.nq += 1;
     if constexpr (WL > 0) return wball_descend<D, WL>(S, q, 0, bound, m, hit, wk);
