@@ -276,9 +276,11 @@ __device__ __forceinline__ bool refill(Queue &q, bool &active, long long &idx, u
 
 // ------------------------------------------------------------------ forward
 // COUNT: the instance that keeps work counters (launched while work
-// accounting is on); the others carry none.
+// accounting is on); the others carry none.  The 3D instances are compiled
+// for 3 resident blocks of 512 (a 40-register cap): 1 % faster than 2 blocks
+// at 64 registers; the 2D ones stay at 64 registers.
 template <int D, bool BVH, bool RECORDS, int WL, bool COUNT>
-__global__ void __launch_bounds__(512) k_walk(SceneView S, WalkCfg c, const float *__restrict__ P, long long total,
+__global__ void __launch_bounds__(512, D == 3 ? 3 : 1) k_walk(SceneView S, WalkCfg c, const float *__restrict__ P, long long total,
                                              unsigned long long *counter, int chunk, int n_top, int stage_cdf,
                                              WalkOut out) {
     extern __shared__ float4 smem[];
@@ -749,11 +751,17 @@ __device__ __forceinline__ AdjSmem<D> adj_smem(double *base, bool acc) {
 }
 
 // The adjoint kernel runs at most 256 threads per block and is compiled for
-// at least ADJ_MIN_BLOCKS resident blocks per SM: a 64-register cap.  The 3D
-// kernel spills a little at that cap and is still faster than at 80
-// registers and three blocks.
+// at least ADJ_MIN_BLOCKS resident blocks per SM: a 64-register cap.  The
+// single-scene 3D kernel, whose leaf loads wait on L2, is compiled for
+// ADJ_MIN_BLOCKS_3D (a 40-register cap): measured against 3, 4, 5, 7 and 8
+// blocks it is the fastest despite its spills (4 -> 6: C3 step -3 %; 7 and 8
+// spill far more and lose 10 %).  The 2D kernel is fastest at 4 and the
+// batched kernels, which carry more per-lane state, at 4 in both dimensions.
 #ifndef ADJ_MIN_BLOCKS
 #define ADJ_MIN_BLOCKS 4
+#endif
+#ifndef ADJ_MIN_BLOCKS_3D
+#define ADJ_MIN_BLOCKS_3D 6
 #endif
 
 // Persistent adjoint kernel.  ND_ONLY: the items are boundary records and the
@@ -761,7 +769,7 @@ __device__ __forceinline__ AdjSmem<D> adj_smem(double *base, bool acc) {
 // wos_normal_derivative entry point); otherwise items are (point, walk)
 // samples and gradients are accumulated into dV / dg / dsrc.
 template <int D, bool BVH, int MODE, int WL, bool COUNT>
-__global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint(SceneView S, WalkCfg c, AdjCfg a, const float *__restrict__ P,
+__global__ void __launch_bounds__(256, D == 3 ? ADJ_MIN_BLOCKS_3D : ADJ_MIN_BLOCKS) k_adjoint(SceneView S, WalkCfg c, AdjCfg a, const float *__restrict__ P,
                                                 long long total, const float *__restrict__ dLdu,
                                                 unsigned long long *counter, int chunk, int n_top, int stage_cdf,
                                                 AdjOut out) {
@@ -2186,7 +2194,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
     extern __shared__ float4 smem[];
     // source-gradient accumulators only when the launch has source derivatives
     // (the launcher sizes shared memory the same way)
-    const bool acc_on = wds != nullptr;
+    const bool acc_on = D == 2 && wds != nullptr;  // source derivatives exist in 2D only
     const AdjSmem<D> am = adj_smem<D>(reinterpret_cast<double *>(smem), acc_on);
     AdjSlot<D> &slot = *am.slot;
     double *acc_src = am.acc;  // k-th accumulator at acc_src[k * blockDim.x]
@@ -2253,7 +2261,7 @@ __global__ void __launch_bounds__(256, ADJ_MIN_BLOCKS) k_adjoint_batch(
 #pragma unroll
                     for (int s2 = 0; s2 < D; ++s2) atomicAdd(&acc[it.dg_off + vid[s2]], W * (double)wts[s2]);
                 }
-                if (wds != nullptr && a.want_dsrc && c.include_source && S.src_type != 0) {
+                if (acc_on && a.want_dsrc && c.include_source && S.src_type != 0) {
                     if (acc_item != item) {
                         if (acc_item >= 0) {
 #pragma unroll
