@@ -27,6 +27,12 @@ roofline  the adjoint kernel (the dominant one), which is bound by
         from L1/L2), and `fp32_algorithmic`, the reference algorithm's FP32
         ops (12 per node visit, 20 per segment test, 10 per query) over
         148 SMs x 128 lanes x 2 x SM clock; `traffic` is DRAM bytes.
+other_workloads  after the 2D line is complete (one GPU only; skipped with
+        --no-other-workloads): the 3D forward + adjoint solve on the displaced
+        icosphere at 1,000,000 points x 128 walks, and the 256-scene batch at
+        full scale against the plain per-scene kernel, each timed with its own
+        CUDA events, clocks, accuracy and CPU baseline (the lines that
+        --workload c3 / batched print, without their untimed extras).
 --impl reference  the CPU restatement of the reference algorithm (the
         reference itself cannot run: it needs Dr.Jit/Mitsuba and the lbvh
         submodule), all host threads, bounded samples of the same workload.
@@ -265,10 +271,18 @@ def workload_config(npts):
 
 # ---------------------------------------------------------------- batched workload
 def batched_main(args):
+    print(json.dumps(batched_line(args)), flush=True)
+    return 0
+
+
+def batched_line(args, compact=False):
     """Many scenes in one plan: persistent launches per dimension and tree depth (graph replay):
     seeded random stars and noise-displaced icospheres, harmonic-polynomial
     boundary data, forward + adjoint of mean((u - exact)^2) per scene.
-    Compared with the reference-shaped plain kernel run scene by scene."""
+    Compared with the reference-shaped plain kernel run scene by scene.
+    `compact` (the entry in the default bench line): the tuner times 2 % of
+    each run's walks, brute force runs on every 8th scene instead of every
+    4th, and the per-dimension breakdown plans are left out."""
     import torch
     import wos
     from wos import autotune, shapes
@@ -298,7 +312,7 @@ def batched_main(args):
     plan = wos.BatchPlan(items, adj)
     info = plan.info()
     # per (dimension, phase) slot; large plans time a prefix of each run
-    sample = min(1.0, 0.1 / max(args.scale, 1e-9))
+    sample = min(1.0, (0.02 if compact else 0.1) / max(args.scale, 1e-9))
     slot_best, slot_ms = autotune.tune_batch_slots(plan, sample=sample)
     for _ in range(args.warmup):
         plan.run(use_graph=True)
@@ -328,7 +342,7 @@ def batched_main(args):
     # the reference-shaped plain kernel (one walk per thread, forward only),
     # scene by scene.  Large scenes run on a subsample of >= 2^18 walks (enough
     # to fill the GPU), scaled by points; small scenes run whole.  Brute force
-    # runs on every 4th scene and is extrapolated per dimension by its time
+    # runs on every 4th (compact: 8th) scene and is extrapolated per dimension by its time
     # ratio to the LBVH plain kernel on the same scenes.
     def plain_time(it, use_bvh):
         nw = it.settings.nwalks
@@ -350,7 +364,7 @@ def batched_main(args):
     plain_by_dim = {}
     for dim in (2, 3):
         idx = [i for i, it in enumerate(items) if it.scene.dim == dim]
-        sub = idx[::4]
+        sub = idx[::8 if compact else 4]
         ratio = sum(plain_time(items[i], False) for i in sub) / sum(t_lbvh[i] for i in sub)
         t_brute_est += ratio * sum(t_lbvh[i] for i in idx)
         npts = sum(items[i].points.shape[0] for i in idx)
@@ -373,7 +387,7 @@ def batched_main(args):
         return a.elapsed_time(b)
 
     breakdown = {}
-    for dim in (2, 3):
+    for dim in ((2, 3) if not compact else ()):
         sub = [it for it in items if it.scene.dim == dim]
         breakdown[f"{dim}d"] = {"scenes": len(sub), "walks": sum(it.points.shape[0] * it.settings.nwalks for it in sub),
                                 "forward_ms": plan_ms(sub, None), "forward_adjoint_ms": plan_ms(sub, adj)}
@@ -403,13 +417,14 @@ def batched_main(args):
         "accuracy": {"rmse_vs_exact": (err2 / npts) ** 0.5, "rms_standard_error": (se2 / npts) ** 0.5},
         "device_status": wos.device_status(),
     }
+    if compact:
+        del line["breakdown"]
     if clk is not None:
         line["clocks"] = clk
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = batched_cpu_baseline(scenes, items, exact)
-    print(json.dumps(line), flush=True)
     plan.close()
-    return 0
+    return line
 
 
 def batched_cpu_baseline(scenes, items, exact, every=8, m=4):
@@ -475,12 +490,20 @@ def c3_cpu_baseline(V, F, P, npts, nw, target_s=3.0):
 
 
 def c3_main(args):
+    print(json.dumps(c3_line(args)), flush=True)
+    return 0
+
+
+def c3_line(args, compact=False):
     """The 3D forward + adjoint solve: icosphere subdivided to 81,920
     triangles, radially displaced by 0.15 x seeded 3-octave value noise,
     g = x^2 - y^2 + z, seeded uniform interior points (1,000,000 by default),
     128 walks per point, nsteps 64, epsilon 1e-3; a step is the fused forward
     solve plus the adjoint of mean(u^2) with respect to vertex positions and
-    per-vertex g (epsilon2 1e-3, clamping 0.1)."""
+    per-vertex g (epsilon2 1e-3, clamping 0.1).  `compact` (the entry in the
+    default bench line): the warm-up steps run on 200,000 of the points with
+    16 walks each (the same scene and kernels, a quarter second per step
+    instead of ten), and the untimed work-counting pass is left out."""
     import torch
     import wos
     from wos import shapes
@@ -501,8 +524,10 @@ def c3_main(args):
     def ws(seed):
         return WalkSettings(nwalks=nw, nsteps=64, epsilon=1e-3, seed=seed)
 
+    warm_P, warm_nw = (P[:200_000].contiguous(), min(nw, 16)) if compact else (P, nw)
     for w in range(args.warmup):
-        scene.solve_adjoint(P, ws(100 + w), adj, loss_kind=1)
+        scene.solve_adjoint(warm_P, WalkSettings(nwalks=warm_nw, nsteps=64, epsilon=1e-3, seed=100 + w), adj,
+                            loss_kind=1)
     torch.cuda.synchronize()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     clocks = ClockSampler(None)
@@ -537,15 +562,17 @@ def c3_main(args):
     torch.cuda.synchronize()
     t_plain = a.elapsed_time(b) * 1e-3
     # tree work of one forward solve and one fused step (device counters, untimed)
-    wos.set_work_counting(True)
-    wos.work_counters(reset=True)
-    scene.solve(P, ws(1))
-    torch.cuda.synchronize()
-    fwd_work = wos.work_counters(reset=True)
-    scene.solve_adjoint(P, ws(1), adj, loss_kind=1)
-    torch.cuda.synchronize()
-    fused_work = wos.work_counters(reset=True)
-    wos.set_work_counting(False)
+    fwd_work = fused_work = None
+    if not compact:
+        wos.set_work_counting(True)
+        wos.work_counters(reset=True)
+        scene.solve(P, ws(1))
+        torch.cuda.synchronize()
+        fwd_work = wos.work_counters(reset=True)
+        scene.solve_adjoint(P, ws(1), adj, loss_kind=1)
+        torch.cuda.synchronize()
+        fused_work = wos.work_counters(reset=True)
+        wos.set_work_counting(False)
     walks = npts * nw
     line = {
         "metric": "wos_walks_per_s", "value": walks * args.steps / t, "unit": "walks/s", "n_gpus": 1,
@@ -566,12 +593,14 @@ def c3_main(args):
         "walk_steps": walk_steps(steps, 64),
         "device_status": wos.device_status(),
     }
+    if compact:
+        del line["tree_work"]
+        line["warmup_workload"] = f"{int(warm_P.shape[0])} of the points x {warm_nw} walks"
     if clk is not None:
         line["clocks"] = clk
     if not args.no_cpu_baseline:
         line.update(c3_cpu_baseline(V, F, P.cpu().numpy(), npts, nw))
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 # ---------------------------------------------------------------- inverse workload
@@ -869,6 +898,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-other-workloads", action="store_true",
+                    help="leave the 3D and batched entries out of the default 2D line")
     ap.add_argument("--ref-step-s", type=float, default=6.0)
     ap.add_argument("--grid", type=int, default=GRID, help="query grid (smaller only for profiling captures)")
     ap.add_argument("--walks", type=int, default=None,
@@ -1115,11 +1146,41 @@ def main():
         }
         line["roofline"]["fp32_algorithmic"] = {"achieved_tflops": adj_ops / adj_avg / 1e12,
                                                 "peak_tflops": fp32_peak / 1e12, "frac": adj_ops / adj_avg / fp32_peak}
+    if rank == 0 and world == 1 and not args.no_other_workloads:
+        line["other_workloads"] = other_workloads(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def other_workloads(args):
+    """The configured 3D and batched workloads, run after the 2D step's line
+    is complete and reported beside it (one GPU): the displaced icosphere at
+    1,000,000 points x 128 walks, and the 256-scene batch at full scale, each
+    with its own warm-up, CUDA-event timing, clocks, accuracy against the exact
+    solutions and CPU baseline.  Neither touches the 2D line's figures."""
+    import gc
+    import torch
+    out = {}
+    jobs = (("c3_3d_forward_adjoint", c3_line, dict(points=1_000_000, walks=128, steps=2, warmup=3)),
+            ("c5_batched", batched_line, dict(scale=1.0, steps=1, warmup=1)))
+    for name, fn, kw in jobs:
+        ns = argparse.Namespace(**{**vars(args), **kw})
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn(ns, compact=True)
+        except Exception as e:  # the 2D line is printed whatever happens here
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["wall_s"] = round(time.perf_counter() - t0, 1)
+        gc.collect()
+        try:
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+        except Exception:
+            pass
+    return out
 
 
 def fused_step_launches(nF: int) -> int:
