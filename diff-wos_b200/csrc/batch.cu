@@ -35,6 +35,7 @@ struct BatchGroup {
     std::vector<SceneView> views;
     std::vector<WalkCfg> cfgs;
     std::vector<wos_scene_t> scenes;
+    std::vector<unsigned long long> gens;  // each scene's generation when `views` was read
     long long walks = 0;
     int points = 0;
     bool has_src = false;
@@ -99,11 +100,25 @@ static void drop_graph(wos_batch_s *b) {
 
 static int upload_views(wos_batch_s *b, cudaStream_t st) {
     for (BatchGroup &g : b->groups) {
-        for (size_t i = 0; i < g.scenes.size(); ++i) g.views[i] = g.scenes[i]->impl.view();
+        g.gens.resize(g.scenes.size());
+        for (size_t i = 0; i < g.scenes.size(); ++i) {
+            g.views[i] = g.scenes[i]->impl.view();
+            g.gens[i] = g.scenes[i]->impl.generation;
+        }
         BT(cudaMemcpyAsync(g.d_views, g.views.data(), sizeof(SceneView) * g.views.size(), cudaMemcpyHostToDevice, st));
     }
     BT(cudaStreamSynchronize(st));
     return 0;
+}
+
+// True when a scene of the plan was rebuilt (wos_scene_update_vertices) or
+// given a new source since its view was read: the view's by-value fields
+// (bounding box, extents, source) are then out of date.
+static bool stale_views(const wos_batch_s *b) {
+    for (const BatchGroup &g : b->groups)
+        for (size_t i = 0; i < g.scenes.size(); ++i)
+            if (i >= g.gens.size() || g.gens[i] != g.scenes[i]->impl.generation) return true;
+    return false;
 }
 
 static void set_count_work(wos_batch_s *b, int count) {
@@ -506,6 +521,12 @@ int wos_batch_refresh(wos_batch_t b, wos_stream_t stream) {
 int wos_batch_run(wos_batch_t b, int use_graph, wos_stream_t stream) {
     if (b == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "batch is NULL");
     cudaStream_t st = (cudaStream_t)stream;
+    // scenes changed since their views were read are read again, and the
+    // graph that holds the old views is captured anew
+    if (stale_views(b)) {
+        drop_graph(b);
+        if (int rc = upload_views(b, st)) return rc;
+    }
     // the work-counting flag is a kernel argument: a captured graph keeps the
     // value it was captured with, so a change forces a new capture
     const int count = work_counting_enabled();

@@ -189,6 +189,7 @@ int wos_scene_set_source(wos_scene_t scene, int source_type, const float *params
     if (source_type != 0 && params == nullptr) return fail(WOS_ERR_INVALID_ARGUMENT, "params is NULL");
     S.src_type = source_type;
     for (int k = 0; k < 5; ++k) S.src[k] = source_type ? params[k] : 0.0f;
+    ++S.generation;
     return 0;
 }
 

@@ -727,6 +727,7 @@ void SceneImpl::release(cudaStream_t st) {
     wt_box = nullptr;
     wt_slab = nullptr;
     wt_obb = nullptr;
+    wt_n[0] = wt_n[1] = wt_n[2] = 0;
     guide = nullptr;
 }
 
@@ -874,16 +875,25 @@ static int build_geometry(SceneImpl &S, cudaStream_t st) {
             ++level;
         }
         S.wt_levels = level;
-        if (S.wt_box) cudaFreeAsync(S.wt_box, st);
-        S.wt_box = nullptr;
-        WOS_TRY(dalloc(&S.wt_box, (size_t)off * W, st));
-        if (S.wt_slab) cudaFreeAsync(S.wt_slab, st);
-        S.wt_slab = nullptr;
-        if (S.wt_obb) cudaFreeAsync(S.wt_obb, st);
-        S.wt_obb = nullptr;
+        // The level sizes depend on nF alone, so a rebuild after the vertices
+        // move (wos_scene_update_vertices) refills the buffers of the first
+        // build in place: device views held elsewhere (batch plans, captured
+        // graphs, launches on other streams) keep pointing at live memory.
         const bool slab2 = D == 3 && S.wt_levels >= 2;
-        WOS_TRY(dalloc(&S.wt_slab, slab2 ? (size_t)S.wt_count[2] : 0, st));
-        WOS_TRY(dalloc(&S.wt_obb, (size_t)S.wt_count[1] * (D == 2 ? 2 : 3), st));
+        const size_t n_box = (size_t)off * W, n_slab = slab2 ? (size_t)S.wt_count[2] : 0,
+                     n_obb = (size_t)S.wt_count[1] * (D == 2 ? 2 : 3);
+        if (S.wt_box == nullptr || S.wt_n[0] != n_box || S.wt_n[1] != n_slab || S.wt_n[2] != n_obb) {
+            if (S.wt_box) cudaFreeAsync(S.wt_box, st);
+            if (S.wt_slab) cudaFreeAsync(S.wt_slab, st);
+            if (S.wt_obb) cudaFreeAsync(S.wt_obb, st);
+            S.wt_box = S.wt_slab = S.wt_obb = nullptr;
+            WOS_TRY(dalloc(&S.wt_box, n_box, st));
+            WOS_TRY(dalloc(&S.wt_slab, n_slab, st));
+            WOS_TRY(dalloc(&S.wt_obb, n_obb, st));
+            S.wt_n[0] = n_box;
+            S.wt_n[1] = n_slab;
+            S.wt_n[2] = n_obb;
+        }
         k_wt_level1<D><<<nblk(S.wt_count[1], TB), TB, 0, st>>>(skeys, nF, pbox, S.wt_box, S.wt_count[1]);
         k_wt_obb<D><<<nblk(S.wt_count[1], 64), 64, 0, st>>>(S.lseg, S.ltri, nF, S.wt_obb, S.wt_count[1]);
         for (int l = 2; l <= S.wt_levels; ++l)
@@ -998,7 +1008,11 @@ int SceneImpl::check_indices(cudaStream_t st) {
     return 0;
 }
 
-int SceneImpl::build(cudaStream_t st) { return dim == 2 ? build_geometry<2>(*this, st) : build_geometry<3>(*this, st); }
+int SceneImpl::build(cudaStream_t st) {
+    const int rc = dim == 2 ? build_geometry<2>(*this, st) : build_geometry<3>(*this, st);
+    ++generation;
+    return rc;
+}
 
 SceneView SceneImpl::view() const {
     SceneView v{};

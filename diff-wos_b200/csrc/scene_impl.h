@@ -56,6 +56,11 @@ struct SceneImpl {
     float4 *wt_box = nullptr;
     float4 *wt_slab = nullptr;
     float4 *wt_obb = nullptr;
+    size_t wt_n[3] = {0, 0, 0};  // float4 counts allocated for wt_box, wt_slab, wt_obb
+    // Incremented by every build and source change: the by-value fields of
+    // view() (bounding box, extents, source) may have changed since a view
+    // was taken.
+    unsigned long long generation = 0;
 
     int allocate(cudaStream_t st);
     int check_indices(cudaStream_t st);

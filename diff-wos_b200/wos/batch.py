@@ -97,6 +97,9 @@ class BatchPlan:
         return tuple(int(x) for x in out)
 
     def refresh(self):
+        """Re-read the scenes' device views now.  run() does this by itself
+        for scenes whose vertices (NativeScene.update_vertices) or source
+        changed since the last step, so this is rarely needed."""
         call("wos_batch_refresh", self.h, stream())
 
     def run(self, use_graph=True):

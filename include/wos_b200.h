@@ -149,7 +149,10 @@ WOS_API int wos_scene_destroy(wos_scene_t scene, wos_stream_t stream);
 WOS_API int wos_scene_update_values(wos_scene_t scene, const float *g, wos_stream_t stream);
 
 /* Replace vertex positions (nV x dim, device) and rebuild normals, AABB and
- * LBVH; returns after the rebuild. */
+ * LBVH; returns after the rebuild.  The scene's device buffers stay where they
+ * are (the trees are refilled in place), so batch plans and launches that hold
+ * the scene keep reading live memory; kernels still running on another stream
+ * race with the rebuild and must be ordered before it by the caller. */
 WOS_API int wos_scene_update_vertices(wos_scene_t scene, const float *V, wos_stream_t stream);
 
 /* Set the analytic source (include/scene.cuh:270-301): type 0 none,
@@ -440,7 +443,10 @@ WOS_API int wos_batch_set_launch_slot(wos_batch_t b, int dim, int phase, int blo
  * per block, out[1] blocks per SM (0 = occupancy limit), out[2] chunk. */
 WOS_API int wos_batch_get_launch(wos_batch_t b, int dim, int phase, int32_t *out);
 
-/* Re-read the scenes' device views (after wos_scene_update_vertices). */
+/* Re-read the scenes' device views.  wos_batch_run does this by itself for
+ * scenes rebuilt (wos_scene_update_vertices) or given a new source
+ * (wos_scene_set_source) since the last read, and then captures its graph
+ * anew; this call forces it. */
 WOS_API int wos_batch_refresh(wos_batch_t b, wos_stream_t stream);
 
 /* Run one step.  use_graph != 0: the step is captured once into a CUDA graph

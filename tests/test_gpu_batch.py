@@ -16,9 +16,16 @@ pytestmark = pytest.mark.gpu
 def _items():
     import torch
     from wos import shapes
-    from wos.native import NativeScene, WalkSettings
+    from wos.native import NativeScene as _Native
+    from wos.native import WalkSettings
     rng = np.random.default_rng(0)
     items = []
+
+    def NativeScene(V, F, *a):  # noqa: N802 -- keeps the input vertices beside the scene
+        ns = _Native(V, F, *a)
+        ns.V0 = np.asarray(V, np.float32)
+        return ns
+
     V, F = shapes.circle(512)
     items.append((NativeScene(V, F, shapes.harmonic_c1(V).astype(np.float32)),
                   rng.uniform(-0.6, 0.6, (700, 2)), WalkSettings(nwalks=32, nsteps=64, seed=1), 1))
@@ -167,4 +174,36 @@ def test_slot_tuner_picks_shapes_per_dimension_and_phase(cuda):
         m, dg = ref[i]
         assert np.array_equal(_np(plan.outputs(i)["mean"]), m), i
         np.testing.assert_allclose(_np(plan.outputs(i)["dg"]), dg, rtol=1e-5, atol=1e-7 * np.abs(dg).max())
+    plan.close()
+
+
+def test_plan_follows_scene_updates_without_refresh(cuda):
+    """A plan keeps the scenes it was built from: after their vertices move
+    (wos_scene_update_vertices rebuilds the trees in their buffers) or their
+    source changes, the next run -- graph replay included, no explicit
+    refresh -- equals single-scene calls on the changed scenes."""
+    import torch
+    from wos import BatchItem, BatchPlan
+    from wos.native import AdjointSettings
+    a = AdjointSettings(epsilon2=1e-3, clamping=0.1, want_dV=True, want_dg=True, want_dsrc=True)
+    items = _items()
+    plan = BatchPlan([BatchItem(sc, P, s, kind, tg) for sc, P, s, kind, tg in items], a)
+    plan.run(use_graph=True)
+    before = _np(plan.outputs(0)["mean"]).copy()
+    for i, f in ((0, 1.1), (2, 1.05), (3, 1.08)):
+        sc = items[i][0]
+        sc.update_vertices(torch.as_tensor(sc.V0 * f, device="cuda"))
+    items[1][0].set_source(2, [0.5, -1.0, 0.2, 0.3, 2.0])
+    for _ in range(2):
+        plan.run(use_graph=True)
+        for i, (sc, P, s, kind, tg) in enumerate(items):
+            o = plan.outputs(i)
+            r = sc.solve_adjoint(P, s, a, loss_kind=kind, target=tg, want_var=True)
+            assert np.array_equal(_np(o["mean"]), _np(r["mean"])), i
+            for k in ("dV", "dg", "dsrc"):
+                x, y = _np(o[k]), _np(r[k])
+                np.testing.assert_allclose(x, y, rtol=1e-4, atol=1e-6 * max(np.abs(y).max(), 1e-12)), (i, k)
+    assert not np.array_equal(before, _np(plan.outputs(0)["mean"]))
+    import wos
+    assert wos.device_status() == 0
     plan.close()
