@@ -94,6 +94,20 @@ __device__ __forceinline__ Hit warp_queries(const SceneView &S, bool active, con
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     unsigned act = __ballot_sync(FULL, active);
+    // The per-point parts of each search -- the pruning tolerance (or the
+    // ball's bound) and the warm candidate's distance -- are computed by every
+    // lane for its own point at once, not by the whole warp once per query;
+    // the values are the same bits either way.
+    float lim = 0.0f, wd2 = INFINITY;
+    if (active) {
+        const float tol2 = prune_tol2<D>(S, x);
+        if (ball_m > 0.0f) {
+            lim = wball_bound(ball_m, tol2);
+        } else {
+            lim = tol2;
+            if (warm >= 0) wd2 = prim_d2<D>(S, warm, x);
+        }
+    }
     while (act) {
         const int j = __ffs(act) - 1;
         act &= act - 1u;
@@ -103,15 +117,17 @@ __device__ __forceinline__ Hit warp_queries(const SceneView &S, bool active, con
         q[2] = D == 3 ? __shfl_sync(FULL, x[2], j) : 0.0f;
         const int wp = __shfl_sync(FULL, warm, j);
         const float bm = __shfl_sync(FULL, ball_m, j);
+        const float lj = __shfl_sync(FULL, lim, j);
+        const float wj = __shfl_sync(FULL, wd2, j);
         Hit h{-1, INFINITY};
         if (bm > 0.0f) {
-            wball<D, WL>(S, q, bm, h, work);
+            wball_b<D, WL>(S, q, lj, bm, h, work);
         } else {
             if (wp >= 0) {
                 h.prim = wp;
-                h.d2 = prim_d2<D>(S, wp, q);
+                h.d2 = wj;
             }
-            h = wquery<D, WL>(S, q, h, work);
+            h = wquery_tol<D, WL>(S, q, h, lj, work);
         }
         if (lane == j) mine = h;
     }
@@ -2031,6 +2047,19 @@ __device__ __forceinline__ Hit warp_queries_batch(const SceneView *__restrict__ 
     const int lane = threadIdx.x & 31;
     Hit mine{-1, INFINITY};
     unsigned act = __ballot_sync(FULL, active);
+    // per-point parts of each search, every lane for its own point at once
+    // (as in warp_queries)
+    float lim = 0.0f, wd2 = INFINITY;
+    if (active) {
+        const SceneView &Si = views[item];
+        const float tol2 = prune_tol2<D>(Si, x);
+        if (ball_m > 0.0f) {
+            lim = wball_bound(ball_m, tol2);
+        } else {
+            lim = tol2;
+            if (warm >= 0) wd2 = prim_d2<D>(Si, warm, x);
+        }
+    }
     while (act) {
         const int j = __ffs(act) - 1;
         act &= act - 1u;
@@ -2041,16 +2070,18 @@ __device__ __forceinline__ Hit warp_queries_batch(const SceneView *__restrict__ 
         const int wp = __shfl_sync(FULL, warm, j);
         const int it = __shfl_sync(FULL, item, j);
         const float bm = __shfl_sync(FULL, ball_m, j);
+        const float lj = __shfl_sync(FULL, lim, j);
+        const float wj = __shfl_sync(FULL, wd2, j);
         const SceneView &Sj = views[it];
         Hit h{-1, INFINITY};
         if (bm > 0.0f) {
-            wball<D, WL>(Sj, q, bm, h, work);
+            wball_b<D, WL>(Sj, q, lj, bm, h, work);
         } else {
             if (wp >= 0) {
                 h.prim = wp;
-                h.d2 = prim_d2<D>(Sj, wp, q);
+                h.d2 = wj;
             }
-            h = wquery<D, WL>(Sj, q, h, work);
+            h = wquery_tol<D, WL>(Sj, q, h, lj, work);
         }
         if (lane == j) mine = h;
     }

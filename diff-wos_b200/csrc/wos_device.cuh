@@ -672,10 +672,11 @@ __device__ __forceinline__ void wdescend(const SceneView &S, const float *q, int
 }
 
 // WL > 0: the tree has exactly WL levels (a kernel compiled for one depth
-// holds one descent, which keeps its code small); WL = 0: any depth.
+// holds one descent, which keeps its code small); WL = 0: any depth.  tol2
+// is prune_tol2<D>(S, q), passed in so that a warp can compute it for all its
+// lanes' points at once.
 template <int D, int WL = 0, class WK>
-__device__ __forceinline__ Hit wquery(const SceneView &S, const float *q, Hit best, WK &wk) {
-    const float tol2 = prune_tol2<D>(S, q);
+__device__ __forceinline__ Hit wquery_tol(const SceneView &S, const float *q, Hit best, float tol2, WK &wk) {
     wk.nq += 1;
     if constexpr (WL > 0) {
         wdescend<D, WL>(S, q, 0, tol2, best, wk);
@@ -689,6 +690,11 @@ __device__ __forceinline__ Hit wquery(const SceneView &S, const float *q, Hit be
         default: wdescend<D, 5>(S, q, 0, tol2, best, wk); break;
     }
     return best;
+}
+
+template <int D, int WL = 0, class WK>
+__device__ __forceinline__ Hit wquery(const SceneView &S, const float *q, Hit best, WK &wk) {
+    return wquery_tol<D, WL>(S, q, best, prune_tol2<D>(S, q), wk);
 }
 
 // ------------------------------------------------------------------ ball test
@@ -743,9 +749,13 @@ __device__ __forceinline__ bool wball_descend(const SceneView &S, const float *q
 // at q: returns true with a blocking primitive in `hit`, or false when no
 // primitive blocks.  Boxes are pruned against m^2 with the nearest search's
 // conservative tolerance, so no blocking primitive is missed.
+__device__ __forceinline__ float wball_bound(float m, float tol2) {
+    return wt_bound((m * m) * (1.0f + 0x1p-20f), tol2);
+}
+
+// wball with its pruning bound wball_bound(m, prune_tol2<D>(S, q)) passed in.
 template <int D, int WL = 0, class WK>
-__device__ __forceinline__ bool wball(const SceneView &S, const float *q, float m, Hit &hit, WK &wk) {
-    const float bound = wt_bound((m * m) * (1.0f + 0x1p-20f), prune_tol2<D>(S, q));
+__device__ __forceinline__ bool wball_b(const SceneView &S, const float *q, float bound, float m, Hit &hit, WK &wk) {
     wk.nq += 1;
     if constexpr (WL > 0) return wball_descend<D, WL>(S, q, 0, bound, m, hit, wk);
     switch (S.wt_levels) {
@@ -755,6 +765,11 @@ __device__ __forceinline__ bool wball(const SceneView &S, const float *q, float 
         case 4: return wball_descend<D, 4>(S, q, 0, bound, m, hit, wk);
         default: return wball_descend<D, 5>(S, q, 0, bound, m, hit, wk);
     }
+}
+
+template <int D, int WL = 0, class WK>
+__device__ __forceinline__ bool wball(const SceneView &S, const float *q, float m, Hit &hit, WK &wk) {
+    return wball_b<D, WL>(S, q, wball_bound(m, prune_tol2<D>(S, q)), m, hit, wk);
 }
 
 // ------------------------------------------------------------------ records
