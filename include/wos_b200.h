@@ -400,7 +400,9 @@ typedef struct wos_batch_s *wos_batch_t;
  * walk phase runs one persistent work-queue launch per run of equal depth
  * (compiled for that depth), the reductions one launch per group.
  * wos_batch_info reports the number of groups (dimensions present).
- * Buffers for all outputs are owned by the plan (wos_batch_outputs).  This
+ * Buffers for all outputs are owned by the plan (wos_batch_outputs).  The
+ * plan reads the items' scenes, points and targets in place at every run:
+ * they must outlive it (destroy the plan before its scenes).  This
  * is the batched form of wos_solve_adjoint; no counterpart in the reference,
  * whose callers loop over scenes with one thrust launch each
  * (include/wos.cuh:407-440). */
