@@ -70,3 +70,29 @@ def test_batched_cpu_baseline_small(bench, oracle):
         exact.append(shapes.harmonic_poly(P, sc["coeffs"], sc["degree"]))
     out = bench.batched_cpu_baseline(scenes, items, exact, every=1, m=2)
     assert out["value"] > 0 and out["unit"] == "points/s"
+
+
+def test_other_workloads_report_each_entry_and_survive_a_failure(bench, monkeypatch):
+    """The 3D and batched entries of the default line run at their configured
+    sizes with their own step counts, and a failing entry is reported as an
+    error without losing the other one (the 2D line is printed either way)."""
+    import argparse
+    seen = {}
+
+    def fake_c3(ns, compact=False):
+        seen["c3"] = (ns.points, ns.walks, ns.steps, ns.warmup, compact)
+        return {"value": 1.0}
+
+    def fake_batched(ns, compact=False):
+        seen["batched"] = (ns.scale, ns.steps, ns.warmup, compact)
+        raise RuntimeError("no memory")
+
+    monkeypatch.setattr(bench, "c3_line", fake_c3)
+    monkeypatch.setattr(bench, "batched_line", fake_batched)
+    args = argparse.Namespace(steps=20, warmup=5, points=7, walks=None, scale=0.1, no_cpu_baseline=False)
+    out = bench.other_workloads(args)
+    assert seen["c3"] == (1_000_000, 128, 2, 3, True)
+    assert seen["batched"] == (1.0, 1, 1, True)
+    assert out["c3_3d_forward_adjoint"]["value"] == 1.0
+    assert out["c5_batched"]["error"] == "RuntimeError: no memory"
+    assert all("wall_s" in v for v in out.values())
