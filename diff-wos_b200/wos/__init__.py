@@ -13,7 +13,7 @@ from ._lib import (WosError, device_status, get_launch_config, set_launch_config
 from .scene import BoundarySamplingRecord, ClosestPointRecord, Detector, Intersection, Polyline
 from .scene3d import ClosestPointRecord3D, Detector3D, Detector3DY, Scene3D
 from .solver import ControlVarianceType, CustomSolver, Sampler, Solver
-from .stats import Statistics
+from .stats import Statistics, merge_solves
 from .wos import Baseline, WoS, WoSCUDA
 from .wos3d import WoS3D, WoS3DCUDA
 from .wos_grad import Ours, OursCUDA
@@ -28,5 +28,5 @@ __all__ = [
     "Scene3D", "Solver", "Statistics", "WoS", "WoS3D", "WoS3DCUDA", "WoSCUDA", "WoSWithSource", "WoSWithSourceCUDA",
     "Baseline", "WosError", "device_status", "get_launch_config", "set_launch_config", "set_sample_order",
     "set_work_counting",
-    "work_counters", "shapes", "BatchItem", "BatchPlan", "WoSBoundary", "Baseline2", "Baseline2CUDA", "Baseline23D", "Baseline3D",
+    "work_counters", "merge_solves", "shapes", "BatchItem", "BatchPlan", "WoSBoundary", "Baseline2", "Baseline2CUDA", "Baseline23D", "Baseline3D",
 ]

@@ -139,6 +139,28 @@ def test_statistics():
     assert np.isclose(st.var(x)[-1], x.var())
 
 
+def test_merge_solves_equals_one_solve_of_all_walks(oracle):
+    """A solve resumed over the next walk range: merging the per-point
+    (mean, var) of walks [0, a) and [a, a + b) gives the reduction of all
+    a + b walks (the oracle's reduction, the GPU k_reduce's restatement)."""
+    import torch
+    from wos import merge_solves
+    rng = np.random.default_rng(5)
+    vals = (rng.normal(size=(300, 96)) * rng.uniform(0.1, 3.0, (300, 1)) + 2.0).astype(np.float32)
+    for a in (1, 17, 48, 95):
+        ma, va = oracle.reduce(np.ascontiguousarray(vals[:, :a]))
+        mb, vb = oracle.reduce(np.ascontiguousarray(vals[:, a:]))
+        m, v = merge_solves(ma, va, a, mb, vb, 96 - a)
+        mall, vall = oracle.reduce(vals)
+        np.testing.assert_allclose(m, mall, rtol=1e-12, atol=1e-12)
+        np.testing.assert_allclose(v, vall, rtol=1e-10, atol=1e-12)
+        mt, vt = merge_solves(torch.tensor(ma), torch.tensor(va), a, torch.tensor(mb), torch.tensor(vb), 96 - a)
+        np.testing.assert_allclose(mt.numpy(), m, rtol=1e-15)
+        np.testing.assert_allclose(vt.numpy(), v, rtol=1e-15)
+    m, v = merge_solves(np.zeros(3), np.zeros(3), 0, mall[:3], vall[:3], 96)
+    assert np.array_equal(m, mall[:3]) and np.array_equal(v, vall[:3])
+
+
 @pytest.mark.parametrize("dim,degree", [(2, 1), (2, 3), (3, 1), (3, 2), (3, 3)])
 def test_harmonic_basis_is_harmonic(dim, degree):
     from wos import shapes
